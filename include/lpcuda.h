@@ -1,0 +1,184 @@
+/*
+ * lpcuda.h -- C ABI of the B200 photon-transport library (liblpcuda.so).
+ *
+ * Drop-in boundary for the hot path of LightPropagation: the OpenCL kernel
+ * MCLightPropagation (src/Simulation/MCLightPropagation.cl:1262-1269) and the
+ * launcher class that feeds it (src/Simulation/CalculatePropagation.hpp:212-388).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only; every call returns an int status
+ *     (LP_OK == 0, the reference's SUCCESS, CalculatePropagation.cpp:23-25).
+ *     Nothing is thrown across the ABI.  lp_last_error() gives the message.
+ *   - Inputs are deep-copied at set time (like the reference setters,
+ *     CalculatePropagation.cpp:351-667); the caller keeps ownership of its arrays.
+ *   - Output arrays returned by lp_get_tallies() are owned by the context and stay
+ *     valid until the next lp_run, lp_run_async, lp_zero_tallies or lp_destroy
+ *     on that context.
+ *   - One context per host thread; calls on one context must be serialised.
+ *     Each context owns one CUDA stream.
+ *   - Tallies are unsigned 64-bit fixed point, LP_FIX_ONE units per unit photon
+ *     weight, so sums are exact and identical from run to run and for any grid or
+ *     block shape.
+ */
+#ifndef LPCUDA_H
+#define LPCUDA_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LP_OK            0
+#define LP_ERR_INVALID   1  /* bad argument                                  */
+#define LP_ERR_CUDA      2  /* CUDA runtime error                            */
+#define LP_ERR_STATE     3  /* call out of order (e.g. run before set_mesh)  */
+#define LP_ERR_NOMEM     4  /* allocation failed                             */
+#define LP_ERR_RANGE     5  /* size beyond a supported maximum               */
+#define LP_ERR_TIMEOUT   6  /* a device-side wait gave up                    */
+
+#define LP_FIX_ONE 4294967296.0 /* 2^32 */
+
+/* Reference behaviours kept by default (deterministic quirks of the reference). */
+#define LP_COMPAT_EXIT_RSP       0x1u /* exit weight times (1-Rsp), MCLightPropagation.cl:1000-1008  */
+#define LP_COMPAT_AXIS_NORMAL    0x2u /* normal := +-eZ within 0.01 of the axis, .cl:1493-1498      */
+#define LP_COMPAT_SIGNED_FRESNEL 0x4u /* Fresnel with the signed incidence cosine, .cl:889-896      */
+#define LP_COMPAT_ALL            0x7u
+
+/* Counter slots of lp_tallies.counters */
+enum {
+    LP_C_SCATTER = 0, LP_C_BOUNDARY, LP_C_QUERY, LP_C_ROULETTE, LP_C_MISS, LP_C_CAPPED,
+    LP_C_RZ_DROP, LP_C_VOX_DROP, LP_C_PHOTONS, LP_C_DRAWS, LP_C_SAFE_SKIP, LP_NCOUNTERS = 16
+};
+
+typedef struct lp_ctx lp_ctx;
+
+/* Tally-image extents derived like CalculatePropagation::InitLogVectors
+ * (CalculatePropagation.cpp:120-243). */
+typedef struct lp_geometry {
+    int32_t dimx, dimy, dimz, dimR, dimAlpha;
+    int32_t sft_nx, sft_ny;   /* SFT image  [-dimx/2, dimx/2] x [-dimy/2, dimy/2] */
+    int32_t rz_nr, rz_nz;     /* r-z image  [-dimR, dimR] x [-dimz, 0]            */
+    int32_t kernel_dimR;
+} lp_geometry;
+
+/* Host copies of the tallies of the last run(s), fixed point (LP_FIX_ONE).  */
+typedef struct lp_tallies {
+    const uint64_t *sft;    /* [sft_ny][sft_nx][3] surf, fetal, trans (GetSFTImage)      */
+    const uint64_t *rtd;    /* [dimAlpha][dimR][3] (GetRTdImage)                          */
+    const uint64_t *rz;     /* [rz_nz][rz_nr][2] absorbed, absorbed/mua (GetArz/PhirzImage) */
+    const uint64_t *vox;    /* [nz][ny][nx] absorbed weight per voxel                     */
+    const uint64_t *rbins;  /* [n_rbins][2] surface, transmitted exit weight by radius    */
+    const uint64_t *region; /* [n_media] absorbed weight per region                       */
+    const uint64_t *det;    /* [n_det][2] sum w, sum w^2 of surface exits per ring        */
+    uint64_t counters[LP_NCOUNTERS];
+    int64_t n_vox, n_rbins, n_region, n_det;
+} lp_tallies;
+
+/* --- context -------------------------------------------------------------- */
+/* Replaces CalculatePropagation::CalculatePropagation + createContext
+ * (CalculatePropagation.cpp:27-79, 1302-1335). */
+int lp_create(lp_ctx **out, int device);
+/* Replaces CalculatePropagation::cleanup + ~CalculatePropagation (CP.cpp:1944-2001, 82-115). */
+void lp_destroy(lp_ctx *ctx);
+/* Last error message of ctx (or of the calling thread when ctx is NULL). */
+const char *lp_last_error(const lp_ctx *ctx);
+
+/* --- inputs --------------------------------------------------------------- */
+/* SetTriangles + SetNormals + SetInnerAndOuterTissueIndices
+ * (CalculatePropagation.cpp:541-667): tri = 9 floats (K, L, M) per triangle,
+ * nrm = 3 floats per triangle (normalised on use), med = (inner, outer) region ids.
+ * Builds the SoA BVH.  n_tri up to 2^27. */
+int lp_set_mesh(lp_ctx *ctx, int64_t n_tri, const float *tri, const float *nrm,
+                const int32_t *med);
+/* SetTissueProperties (CalculatePropagation.cpp:427-451): n, mua, mus, g per region
+ * (the packed float4 layout of the kernel's nMuasG argument).  Up to 64 regions. */
+int lp_set_media(lp_ctx *ctx, int32_t n_media, const float *nmuasg);
+/* SetStartTrajectories + SetStartPoint + SetPOI + SetBasisVectors
+ * (CalculatePropagation.cpp:332-339, 365-380, 760-790): p_start[3], k start
+ * directions (only the first is used, as in the kernel, .cl:429-467) and the
+ * 12 floats POI, eX, eY, eZ (the kernel's e_P0XYZ). */
+int lp_set_source(lp_ctx *ctx, const float *p_start, const float *v_start,
+                  const int32_t *v_occ, int32_t k, const float *ep0xyz);
+/* SetDimensions + SetDetectionGridDimensions + SetFetalTissueID
+ * (CalculatePropagation.cpp:536-539, 716-735, 792-794): model extent, detection
+ * grid (x, y, z, r, phi, rho) and the fetal region id.  Fixes the image extents. */
+int lp_set_tally_grid(lp_ctx *ctx, const float *dimensions, const float *det_grid,
+                      int32_t fetal_id);
+/* SetChanceForRoulette + SetWeightThreshold + SetPixelPerUnitFactor
+ * (CalculatePropagation.cpp:380-397) plus the RNG seed that replaces the
+ * time-seeded ran3 table (PSNR.cpp:98) and the compat switches. */
+int lp_set_params(lp_ctx *ctx, float chance, float w_threshold, float factor,
+                  uint64_t seed, uint32_t compat);
+/* Tallies added by this library (no reference counterpart): voxel absorption grid
+ * in the emitter frame, radial exit bins, ring detectors (n_det annuli r_lo, r_hi). */
+int lp_set_extra_tallies(lp_ctx *ctx, const int32_t *vox_n, const float *vox_d,
+                         int32_t n_rbins, float rbin_dr, int32_t n_det, const float *det_r);
+/* Per-photon step cap (watchdog); photons that reach it are stopped and counted. */
+int lp_set_max_steps(lp_ctx *ctx, int64_t max_steps);
+/* Keep the per-photon float8 exit records of the next runs (RecordFSTxy,
+ * MCLightPropagation.cl:119-130): up to `capacity` photons, indexed by photon id
+ * minus the run's first id. */
+int lp_set_exit_records(lp_ctx *ctx, int64_t capacity);
+
+/* --- run -------------------------------------------------------------------- */
+/* CalculatePropagation::Init + Propagation -> ExecKernel (CP.cpp:2003-2025, 1389-1759):
+ * traces photons [first, first + n) in one persistent launch and adds their tallies.
+ * Blocks until done. */
+int lp_run(lp_ctx *ctx, int64_t first, int64_t n);
+/* As lp_run but returns after the launch is queued on the context's stream. */
+int lp_run_async(lp_ctx *ctx, int64_t first, int64_t n);
+int lp_sync(lp_ctx *ctx);
+/* Clear the accumulated tallies and counters. */
+int lp_zero_tallies(lp_ctx *ctx);
+/* Image extents (InitLogVectors, CP.cpp:120-243). */
+int lp_get_geometry(lp_ctx *ctx, lp_geometry *out);
+/* Copy the tallies to host memory owned by ctx (GetSFTImage / GetRTdImage /
+ * GetArzImage / GetPhirzImage, CalculatePropagation.cpp:897-1056). */
+int lp_get_tallies(lp_ctx *ctx, lp_tallies *out);
+/* Copy n exit records (8 floats each) to out. */
+int lp_get_exit_records(lp_ctx *ctx, float *out, int64_t n);
+/* Device time of the last lp_run* in milliseconds (PrintTimeSpent, CP.cpp:2063-2070). */
+int lp_last_kernel_ms(lp_ctx *ctx, float *ms);
+
+/* Launch and transfer statistics of a context (PrintSimulationParams,
+ * CalculatePropagation.cpp:2043-2048, extended). */
+typedef struct lp_stats {
+    int64_t n_tri, n_nodes;
+    int32_t bvh_depth, nodes_smem, tris_smem, smem_bytes, blocks_per_sm, grid, block, num_sms;
+    int64_t h2d_bytes;      /* bytes uploaded by the last lp_run* (0 if nothing changed) */
+    int64_t d2h_bytes;      /* bytes copied by the last lp_get_tallies                   */
+    float last_kernel_ms;
+} lp_stats;
+int lp_get_stats(lp_ctx *ctx, lp_stats *out);
+
+/* Device addresses of the tally arrays (same layouts as lp_tallies), for a caller
+ * that reduces them across GPUs without a host round trip.  Valid until the next
+ * lp_set_tally_grid / lp_set_extra_tallies / lp_destroy. */
+typedef struct lp_device_tallies {
+    uint64_t *sft, *rtd, *rz, *vox, *rbins, *region, *det, *counters;
+    int64_t n_sft, n_rtd, n_rz, n_vox, n_rbins, n_region, n_det, n_counters;
+    void *stream;            /* the context's cudaStream_t */
+} lp_device_tallies;
+int lp_get_device_tallies(lp_ctx *ctx, lp_device_tallies *out);
+
+/* FP32 FMA throughput of the device in TFLOP/s (2 flops per FMA), measured by a
+ * dependent-FMA kernel: the roofline denominator of the transport kernel. */
+int lp_fp32_peak(int device, double *tflops);
+
+/* --- verification entry points ---------------------------------------------- */
+/* Nearest-triangle queries through the device BVH for n rays (FindTriangleInPath,
+ * MCLightPropagation.cl:1037-1093): origins/dirs 3 floats per ray, ref_tri the
+ * excluded triangle per ray (or -1), t_max the query bound per ray.  Writes the
+ * triangle id (-1 for none) and the distance (10000 for none). */
+int lp_query_triangles(lp_ctx *ctx, int64_t n, const float *orig, const float *dir,
+                       const int32_t *ref_tri, const float *t_max, int32_t *id_out,
+                       float *t_out);
+/* Philox4x32-10 blocks on the device: out[4*i..] = philox(ctr + (0,0,i,0), key). */
+int lp_philox_blocks(int device, const uint32_t *ctr, const uint32_t *key, int64_t n,
+                     uint32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,125 @@
+"""ctypes bindings of liblpcuda.so (the C ABI declared in include/lpcuda.h).
+
+The library is built in-tree by ``lightpropagation_b200.build.build()``.  There is
+no fallback: if the shared library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblpcuda.so")
+
+LP_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "out of memory",
+          5: "size out of range", 6: "device wait timed out"}
+COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL, COMPAT_ALL = 1, 2, 4, 7
+NCOUNTERS = 16
+COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped", "rz_drop",
+                 "vox_drop", "photons", "draws", "safe_skip"]
+FIX_ONE = float(2 ** 32)
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_up = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+
+
+class Geometry(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in
+                ("dimx", "dimy", "dimz", "dimR", "dimAlpha", "sft_nx", "sft_ny",
+                 "rz_nr", "rz_nz", "kernel_dimR")]
+
+
+class Tallies(C.Structure):
+    _fields_ = [("sft", _up), ("rtd", _up), ("rz", _up), ("vox", _up), ("rbins", _up),
+                ("region", _up), ("det", _up), ("counters", C.c_uint64 * NCOUNTERS),
+                ("n_vox", C.c_int64), ("n_rbins", C.c_int64), ("n_region", C.c_int64),
+                ("n_det", C.c_int64)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_tri", C.c_int64), ("n_nodes", C.c_int64)] + \
+        [(n, C.c_int32) for n in ("bvh_depth", "nodes_smem", "tris_smem", "smem_bytes", "blocks_per_sm",
+                                  "grid", "block", "num_sms")] + \
+        [("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("last_kernel_ms", C.c_float)]
+
+
+class DeviceTallies(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("sft", "rtd", "rz", "vox", "rbins", "region", "det", "counters")] + \
+        [(n, C.c_int64) for n in ("n_sft", "n_rtd", "n_rz", "n_vox", "n_rbins", "n_region", "n_det",
+                                  "n_counters")] + [("stream", C.c_void_p)]
+
+
+class LPError(RuntimeError):
+    """Raised when a liblpcuda call returns a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"liblpcuda error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+_SIGS = {
+    "lp_create": ([C.POINTER(C.c_void_p), C.c_int], C.c_int),
+    "lp_destroy": ([C.c_void_p], None),
+    "lp_last_error": ([C.c_void_p], C.c_char_p),
+    "lp_set_mesh": ([C.c_void_p, C.c_int64, _fp, _fp, _ip], C.c_int),
+    "lp_set_media": ([C.c_void_p, C.c_int32, _fp], C.c_int),
+    "lp_set_source": ([C.c_void_p, _fp, _fp, _ip, C.c_int32, _fp], C.c_int),
+    "lp_set_tally_grid": ([C.c_void_p, _fp, _fp, C.c_int32], C.c_int),
+    "lp_set_params": ([C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_uint32], C.c_int),
+    "lp_set_extra_tallies": ([C.c_void_p, _ip, _fp, C.c_int32, C.c_float, C.c_int32, _fp], C.c_int),
+    "lp_set_max_steps": ([C.c_void_p, C.c_int64], C.c_int),
+    "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
+    "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
+    "lp_run_async": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
+    "lp_sync": ([C.c_void_p], C.c_int),
+    "lp_zero_tallies": ([C.c_void_p], C.c_int),
+    "lp_get_geometry": ([C.c_void_p, C.POINTER(Geometry)], C.c_int),
+    "lp_get_tallies": ([C.c_void_p, C.POINTER(Tallies)], C.c_int),
+    "lp_get_exit_records": ([C.c_void_p, _fp, C.c_int64], C.c_int),
+    "lp_last_kernel_ms": ([C.c_void_p, _fp], C.c_int),
+    "lp_query_triangles": ([C.c_void_p, C.c_int64, _fp, _fp, _ip, _fp, _ip, _fp], C.c_int),
+    "lp_philox_blocks": ([C.c_int, _u32p, _u32p, C.c_int64, _u32p], C.c_int),
+    "lp_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "lp_get_device_tallies": ([C.c_void_p, C.POINTER(DeviceTallies)], C.c_int),
+    "lp_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+}
+
+EXPORTED = sorted(_SIGS)
+
+
+def lib():
+    """Load liblpcuda.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.isfile(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with lightpropagation_b200.build.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int, ctx=None) -> None:
+    if rc != LP_OK:
+        msg = lib().lp_last_error(ctx)
+        raise LPError(rc, msg.decode() if msg else "")
+
+
+def fptr(a):
+    return a.ctypes.data_as(_fp)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def u32ptr(a):
+    return a.ctypes.data_as(_u32p)

@@ -1,0 +1,769 @@
+// lp_capi.cu -- C ABI of liblpcuda.so (declared in include/lpcuda.h).
+//
+// Host side of the drop-in for the reference launcher
+// (src/Simulation/CalculatePropagation.cpp): setters copy their inputs, lp_run
+// uploads what changed, launches the persistent transport kernel once for the
+// whole photon budget (the reference loops over 6400-photon launches,
+// CalculatePropagation.cpp:1446-1451) and accumulates fixed-point tallies on the
+// device.  No exceptions cross the ABI; errors are int codes plus a message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lpcuda.h"
+#include "lp_bvh.hpp"
+#include "lp_kernel.cuh"
+
+namespace lp {
+int smem_bytes(int n_media, int nodes_smem, int tris_smem);
+cudaError_t launch_transport(const KParams &P, int grid, int smem, cudaStream_t s);
+cudaError_t transport_occupancy(int smem, int *blocks_per_sm);
+cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *orig, const float *dir,
+                         const int32_t *ref, const float *tmax, int32_t *id_out, float *t_out,
+                         cudaStream_t s);
+cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out,
+                          cudaStream_t s);
+double fma_peak_tflops(int num_sms);
+int block_size();
+}  // namespace lp
+
+using lp::KParams;
+using lp::Medium;
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t count)
+    {
+        if (count <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+struct lp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    int num_sms = 148;
+    // inputs
+    bool have_mesh = false, have_media = false, have_source = false, have_grid = false;
+    bool mesh_dirty = false, media_dirty = false, tally_dirty = true;
+    int64_t n_tri = 0;
+    int32_t max_region = 0;   // largest region id referenced by the mesh
+    lp::Bvh bvh;
+    std::vector<float4> tri_attr;
+    std::vector<float> nmuasg;
+    int32_t n_media = 0;
+    float p_start[3] = {0, 0, 0}, v_start[3] = {0, 0, 1}, ep0xyz[12] = {0};
+    float dimensions[3] = {1, 1, 1}, det_grid[6] = {1, 1, 1, 1, 1, 1};
+    int32_t fetal_id = 1;
+    float chance = 0.1f, w_th = 1e-4f, factor = 1.0f;
+    uint64_t seed = 0x4C50;
+    uint32_t compat = LP_COMPAT_ALL;
+    int64_t max_steps = 100000000;
+    int32_t vox_n[3] = {0, 0, 0};
+    float vox_d[3] = {1, 1, 1};
+    int32_t n_rbins = 0;
+    float rbin_dr = 1.0f;
+    std::vector<float> det_r;
+    int64_t exit_cap = 0;
+    lp_geometry geo{};
+    // device buffers
+    DevBuf<float4> node_a, node_b, node_c, tri_a, tri_b, tri_c, attr;
+    DevBuf<int4> node_d;
+    DevBuf<Medium> media;
+    DevBuf<unsigned long long> sft, rtd, rz, vox, rbins, region, det, counters, work;
+    DevBuf<float> exit_rec;
+    // host copies of tallies
+    std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
+    float last_ms = 0.0f;
+    bool launched = false;
+    // statistics
+    int64_t h2d_bytes = 0, d2h_bytes = 0;
+    int32_t st_nodes_smem = 0, st_tris_smem = 0, st_smem = 0, st_per_sm = 0, st_grid = 0;
+};
+
+namespace {
+
+int fail(lp_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    g_thread_error = buf;
+    return code;
+}
+
+int cuda_fail(lp_ctx *c, cudaError_t e, const char *what)
+{
+    return fail(c, LP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define LP_CUDA(ctx, call)                                   \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+void geometry_of(const float dims[3], const float dg[6], lp_geometry &g)
+{
+    // CalculatePropagation::InitLogVectors (CP.cpp:127-131): float divisions, int casts
+    g.dimx = (int32_t)(dims[0] / dg[0]);
+    g.dimy = (int32_t)(dims[1] / dg[1]);
+    g.dimz = (int32_t)(dims[2] / dg[2]);
+    g.dimAlpha = (int32_t)(90 / dg[5]);
+    g.dimR = (int32_t)std::ceil(std::sqrt(std::pow((double)(g.dimx / 2), 2) + std::pow((double)(g.dimy / 2), 2)));
+    g.sft_nx = 2 * (g.dimx / 2) + 1;
+    g.sft_ny = 2 * (g.dimy / 2) + 1;
+    g.rz_nr = 2 * g.dimR + 1;
+    g.rz_nz = g.dimz + 1;
+    const float hx = (float)g.dimx / 2, hy = (float)g.dimy / 2;
+    g.kernel_dimR = (int32_t)std::ceil(std::sqrt(std::pow(hx, 2.0f) + std::pow(hy, 2.0f)));
+}
+
+inline float normf3(float v[3])
+{
+    float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l != 0.0f) {
+        v[0] = v[0] / l;
+        v[1] = v[1] / l;
+        v[2] = v[2] / l;
+    }
+    return l;
+}
+
+int64_t n_vox(const lp_ctx *c)
+{
+    return c->vox_n[0] > 0 ? (int64_t)c->vox_n[0] * c->vox_n[1] * c->vox_n[2] : 0;
+}
+
+int alloc_tallies(lp_ctx *c)
+{
+    const lp_geometry &g = c->geo;
+    LP_CUDA(c, c->sft.ensure((size_t)g.sft_nx * g.sft_ny * 3));
+    LP_CUDA(c, c->rtd.ensure((size_t)g.dimR * g.dimAlpha * 3));
+    LP_CUDA(c, c->rz.ensure((size_t)g.rz_nr * g.rz_nz * 2));
+    LP_CUDA(c, c->vox.ensure((size_t)std::max<int64_t>(n_vox(c), 1)));
+    LP_CUDA(c, c->rbins.ensure((size_t)std::max(c->n_rbins, 1) * 2));
+    LP_CUDA(c, c->region.ensure(lp::kMaxMedia));
+    LP_CUDA(c, c->det.ensure((size_t)lp::kMaxDet * 2));
+    LP_CUDA(c, c->counters.ensure(LP_NCOUNTERS));
+    LP_CUDA(c, c->work.ensure(1));
+    return LP_OK;
+}
+
+int zero_tallies(lp_ctx *c)
+{
+    const lp_geometry &g = c->geo;
+    cudaStream_t s = c->stream;
+    LP_CUDA(c, cudaMemsetAsync(c->sft.p, 0, (size_t)g.sft_nx * g.sft_ny * 3 * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->rtd.p, 0, (size_t)g.dimR * g.dimAlpha * 3 * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->rz.p, 0, (size_t)g.rz_nr * g.rz_nz * 2 * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->vox.p, 0, (size_t)std::max<int64_t>(n_vox(c), 1) * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->rbins.p, 0, (size_t)std::max(c->n_rbins, 1) * 2 * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->region.p, 0, lp::kMaxMedia * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->det.p, 0, lp::kMaxDet * 2 * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->counters.p, 0, LP_NCOUNTERS * 8, s));
+    return LP_OK;
+}
+
+int upload_mesh(lp_ctx *c)
+{
+    if (!c->mesh_dirty) return LP_OK;
+    const lp::Bvh &b = c->bvh;
+    const size_t nn = b.node_a.size(), nt = b.tri_a.size();
+    LP_CUDA(c, c->node_a.ensure(nn));
+    LP_CUDA(c, c->node_b.ensure(nn));
+    LP_CUDA(c, c->node_c.ensure(nn));
+    LP_CUDA(c, c->node_d.ensure(nn));
+    LP_CUDA(c, c->tri_a.ensure(nt));
+    LP_CUDA(c, c->tri_b.ensure(nt));
+    LP_CUDA(c, c->tri_c.ensure(nt));
+    LP_CUDA(c, c->attr.ensure(nt));
+    cudaStream_t s = c->stream;
+    LP_CUDA(c, cudaMemcpyAsync(c->node_a.p, b.node_a.data(), nn * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->node_b.p, b.node_b.data(), nn * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->node_c.p, b.node_c.data(), nn * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->node_d.p, b.node_d.data(), nn * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->tri_a.p, b.tri_a.data(), nt * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->tri_b.p, b.tri_b.data(), nt * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->tri_c.p, b.tri_c.data(), nt * 16, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->attr.p, c->tri_attr.data(), nt * 16, cudaMemcpyHostToDevice, s));
+    c->h2d_bytes += (int64_t)(nn * 64 + nt * 64);
+    c->mesh_dirty = false;
+    return LP_OK;
+}
+
+int upload_media(lp_ctx *c)
+{
+    if (!c->media_dirty) return LP_OK;
+    std::vector<Medium> m((size_t)c->n_media);
+    for (int i = 0; i < c->n_media; ++i) {
+        const float *q = &c->nmuasg[4 * i];
+        m[i].n = q[0];
+        m[i].mua = q[1];
+        m[i].mus = q[2];
+        m[i].g = q[3];
+        m[i].mut = q[1] + q[2];
+        m[i].alb = q[1] / (q[1] + q[2]);
+        m[i].absorbs = (q[1] > 0.0f && q[2] > 0.0f) ? 1 : 0;
+        m[i].ambient = (q[1] == 0.0f && q[2] == 0.0f) ? 1 : 0;
+    }
+    LP_CUDA(c, c->media.ensure(lp::kMaxMedia));
+    LP_CUDA(c, cudaMemcpyAsync(c->media.p, m.data(), m.size() * sizeof(Medium), cudaMemcpyHostToDevice,
+                               c->stream));
+    c->h2d_bytes += (int64_t)(m.size() * sizeof(Medium));
+    c->media_dirty = false;
+    return LP_OK;
+}
+
+int upload(lp_ctx *c)
+{
+    if (!c->have_mesh || !c->have_media || !c->have_source || !c->have_grid)
+        return fail(c, LP_ERR_STATE, "lp_run: mesh, media, source and tally grid must be set first");
+    if (c->max_region >= c->n_media)
+        return fail(c, LP_ERR_INVALID, "lp_run: mesh references region %d but only %d regions are set",
+                    c->max_region, c->n_media);
+    LP_CUDA(c, cudaSetDevice(c->device));
+    int r = upload_mesh(c);
+    if (r) return r;
+    r = upload_media(c);
+    if (r) return r;
+    if (c->tally_dirty) {
+        r = alloc_tallies(c);
+        if (r) return r;
+        r = zero_tallies(c);
+        if (r) return r;
+        c->tally_dirty = false;
+    }
+    if (c->exit_cap > 0) LP_CUDA(c, c->exit_rec.ensure((size_t)c->exit_cap * 8));
+    return LP_OK;
+}
+
+float rspecular(const float *nm, int n_media)
+{
+    // Rspecular (MCLightPropagation.cl:273-299)
+    if (n_media < 2) return 0.0f;
+    float r1, r2, temp;
+    const float n1 = nm[0], n2 = nm[4], mua1 = nm[5], mus1 = nm[6];
+    temp = (n1 - n2) / (n1 + n2);
+    r1 = temp * temp;
+    if (mua1 == 0.0f && mus1 == 0.0f && n_media > 2) {
+        const float n3 = nm[8];
+        temp = (n2 - n3) / (n2 + n3);
+        r2 = temp * temp;
+        r1 = r1 + (1 - r1) * (1 - r1) * r2 / (1 - r1 * r2);
+    }
+    return r1;
+}
+
+void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem, int tris_smem)
+{
+    std::memset(&P, 0, sizeof P);
+    P.node_a = c->node_a.p; P.node_b = c->node_b.p; P.node_c = c->node_c.p; P.node_d = c->node_d.p;
+    P.tri_a = c->tri_a.p; P.tri_b = c->tri_b.p; P.tri_c = c->tri_c.p; P.tri_attr = c->attr.p;
+    P.n_nodes = (int32_t)c->bvh.node_a.size();
+    P.n_tri = (int32_t)c->n_tri;
+    P.nodes_smem = nodes_smem;
+    P.tris_smem = tris_smem;
+    P.media = c->media.p;
+    P.n_media = c->n_media;
+    P.p0x = c->p_start[0]; P.p0y = c->p_start[1]; P.p0z = c->p_start[2];
+    P.v0x = c->v_start[0]; P.v0y = c->v_start[1]; P.v0z = c->v_start[2];
+    P.poix = c->ep0xyz[0]; P.poiy = c->ep0xyz[1]; P.poiz = c->ep0xyz[2];
+    float ex[3] = {c->ep0xyz[3], c->ep0xyz[4], c->ep0xyz[5]};
+    float ey[3] = {c->ep0xyz[6], c->ep0xyz[7], c->ep0xyz[8]};
+    float ez[3] = {c->ep0xyz[9], c->ep0xyz[10], c->ep0xyz[11]};
+    P.ezx = ez[0]; P.ezy = ez[1]; P.ezz = ez[2];
+    normf3(ex); normf3(ey); normf3(ez);
+    P.nxx = ex[0]; P.nxy = ex[1]; P.nxz = ex[2];
+    P.nyx = ey[0]; P.nyy = ey[1]; P.nyz = ey[2];
+    P.nzx = ez[0]; P.nzy = ez[1]; P.nzz = ez[2];
+    P.Rsp = rspecular(c->nmuasg.data(), c->n_media);
+    P.w0 = 1.0f - P.Rsp;
+    P.exitScale = (c->compat & LP_COMPAT_EXIT_RSP) ? (1 - P.Rsp) : 1.0f;
+    P.distMin = c->det_grid[2] * (float)c->geo.dimz / 2.0f;   // .cl:1351
+    P.chance = c->chance;
+    P.w_th = c->w_th;
+    P.factor = c->factor;
+    P.fetal_id = c->fetal_id;
+    P.compat = c->compat;
+    P.key0 = (uint32_t)c->seed;
+    P.key1 = (uint32_t)(c->seed >> 32);
+    P.stream = 0;
+    P.first = first;
+    P.n = n;
+    P.max_steps = c->max_steps;
+    const lp_geometry &g = c->geo;
+    P.hx = g.dimx / 2; P.hy = g.dimy / 2; P.sft_nx = g.sft_nx;
+    P.dimR = g.dimR; P.dimAlpha = g.dimAlpha; P.rz_nr = g.rz_nr; P.rz_nz = g.rz_nz;
+    for (int i = 0; i < 6; ++i) P.dg[i] = c->det_grid[i];
+    P.sft = c->sft.p; P.rtd = c->rtd.p; P.rz = c->rz.p; P.vox = c->vox.p; P.rbins = c->rbins.p;
+    P.region = c->region.p; P.det = c->det.p; P.counters = c->counters.p;
+    P.vox_nx = c->vox_n[0]; P.vox_ny = c->vox_n[1]; P.vox_nz = c->vox_n[2];
+    P.vox_dx = c->vox_d[0]; P.vox_dy = c->vox_d[1]; P.vox_dz = c->vox_d[2];
+    P.n_rbins = c->n_rbins;
+    P.rbin_dr = c->rbin_dr;
+    P.n_det = (int32_t)(c->det_r.size() / 2);
+    for (int k = 0; k < P.n_det; ++k) {
+        P.det_lo[k] = c->det_r[2 * k];
+        P.det_hi[k] = c->det_r[2 * k + 1];
+    }
+    P.exit_rec = c->exit_cap > 0 ? c->exit_rec.p : nullptr;
+    P.exit_cap = c->exit_cap;
+    P.work = c->work.p;
+}
+
+// shared-memory staging: as many top BVH levels and leading triangles as fit the budget
+void smem_plan(const lp_ctx *c, int budget, int &nodes_smem, int &tris_smem)
+{
+    const int base = lp::smem_bytes(c->n_media, 0, 0);
+    int room = std::max(0, budget - base);
+    const int nn = (int)c->bvh.node_a.size(), nt = (int)c->bvh.tri_a.size();
+    nodes_smem = std::min(nn, room / 64);
+    room -= nodes_smem * 64;
+    tris_smem = std::min(nt, room / 48);
+}
+
+}  // namespace
+
+// ============================================================ C ABI
+extern "C" {
+
+const char *lp_last_error(const lp_ctx *ctx)
+{
+    if (ctx) return ctx->err.c_str();
+    return g_thread_error.c_str();
+}
+
+int lp_create(lp_ctx **out, int device)
+{
+    if (!out) return fail(nullptr, LP_ERR_INVALID, "lp_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(nullptr, LP_ERR_CUDA, "lp_create: no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n) return fail(nullptr, LP_ERR_INVALID, "lp_create: device %d of %d", device, n);
+    lp_ctx *c = new (std::nothrow) lp_ctx;
+    if (!c) return fail(nullptr, LP_ERR_NOMEM, "lp_create: out of host memory");
+    c->device = device;
+    if ((e = cudaSetDevice(device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "lp_create");
+        delete c;
+        return r;
+    }
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return LP_OK;
+}
+
+void lp_destroy(lp_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->node_a.release(); c->node_b.release(); c->node_c.release(); c->node_d.release();
+    c->tri_a.release(); c->tri_b.release(); c->tri_c.release(); c->attr.release();
+    c->media.release();
+    c->sft.release(); c->rtd.release(); c->rz.release(); c->vox.release(); c->rbins.release();
+    c->region.release(); c->det.release(); c->counters.release(); c->work.release();
+    c->exit_rec.release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int lp_set_mesh(lp_ctx *c, int64_t n_tri, const float *tri, const float *nrm, const int32_t *med)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_mesh: ctx is NULL");
+    if (n_tri <= 0 || !tri || !nrm || !med) return fail(c, LP_ERR_INVALID, "lp_set_mesh: empty mesh or NULL array");
+    if (n_tri > (int64_t(1) << 27)) return fail(c, LP_ERR_RANGE, "lp_set_mesh: %lld triangles > 2^27", (long long)n_tri);
+    for (int64_t i = 0; i < 2 * n_tri; ++i)
+        if (med[i] < 0 || med[i] >= lp::kMaxMedia)
+            return fail(c, LP_ERR_INVALID, "lp_set_mesh: region id %d of triangle %lld out of range", med[i],
+                        (long long)(i / 2));
+    lp::build_bvh(tri, n_tri, c->bvh);
+    if (c->bvh.depth >= lp::kStackDepth)
+        return fail(c, LP_ERR_RANGE, "lp_set_mesh: BVH depth %d exceeds the traversal stack", c->bvh.depth);
+    c->tri_attr.resize((size_t)n_tri);
+    for (int64_t i = 0; i < n_tri; ++i) {
+        // nv = normalize(vload3(triID, normals)) (.cl:1489), done once here
+        float v[3] = {nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]};
+        normf3(v);
+        const int32_t ids = (med[2 * i] & 0xffff) | (med[2 * i + 1] << 16);
+        float fb;
+        std::memcpy(&fb, &ids, 4);
+        c->tri_attr[i] = make_float4(v[0], v[1], v[2], fb);
+    }
+    c->n_tri = n_tri;
+    c->max_region = 0;
+    for (int64_t i = 0; i < 2 * n_tri; ++i) c->max_region = std::max(c->max_region, med[i]);
+    c->have_mesh = true;
+    c->mesh_dirty = true;
+    return LP_OK;
+}
+
+int lp_set_media(lp_ctx *c, int32_t n_media, const float *nmuasg)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_media: ctx is NULL");
+    if (n_media < 1 || n_media > lp::kMaxMedia || !nmuasg)
+        return fail(c, LP_ERR_RANGE, "lp_set_media: %d regions (1..%d supported)", n_media, lp::kMaxMedia);
+    for (int i = 0; i < 4 * n_media; ++i)
+        if (!std::isfinite(nmuasg[i])) return fail(c, LP_ERR_INVALID, "lp_set_media: non-finite value at %d", i);
+    c->nmuasg.assign(nmuasg, nmuasg + 4 * n_media);
+    c->n_media = n_media;
+    c->have_media = true;
+    c->media_dirty = true;
+    return LP_OK;
+}
+
+int lp_set_source(lp_ctx *c, const float *p_start, const float *v_start, const int32_t *v_occ, int32_t k,
+                  const float *ep0xyz)
+{
+    (void)v_occ;
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_source: ctx is NULL");
+    if (!p_start || !v_start || k < 1 || !ep0xyz) return fail(c, LP_ERR_INVALID, "lp_set_source: missing input");
+    std::memcpy(c->p_start, p_start, 12);
+    std::memcpy(c->v_start, v_start, 12);
+    std::memcpy(c->ep0xyz, ep0xyz, 48);
+    c->have_source = true;
+    return LP_OK;
+}
+
+int lp_set_tally_grid(lp_ctx *c, const float *dimensions, const float *det_grid, int32_t fetal_id)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_tally_grid: ctx is NULL");
+    if (!dimensions || !det_grid) return fail(c, LP_ERR_INVALID, "lp_set_tally_grid: NULL input");
+    for (int i = 0; i < 6; ++i)
+        if (!(det_grid[i] > 0.0f)) return fail(c, LP_ERR_INVALID, "lp_set_tally_grid: grid step %d not positive", i);
+    lp_geometry g;
+    geometry_of(dimensions, det_grid, g);
+    if (g.dimx < 0 || g.dimy < 0 || g.dimz < 0 || g.dimAlpha < 1 || g.dimR < 1 ||
+        (int64_t)g.sft_nx * g.sft_ny > (int64_t(1) << 28) || (int64_t)g.rz_nr * g.rz_nz > (int64_t(1) << 28))
+        return fail(c, LP_ERR_RANGE, "lp_set_tally_grid: image extents out of range");
+    std::memcpy(c->dimensions, dimensions, 12);
+    std::memcpy(c->det_grid, det_grid, 24);
+    c->geo = g;
+    c->fetal_id = fetal_id;
+    c->have_grid = true;
+    c->tally_dirty = true;
+    return LP_OK;
+}
+
+int lp_set_params(lp_ctx *c, float chance, float w_threshold, float factor, uint64_t seed, uint32_t compat)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_params: ctx is NULL");
+    if (!(chance > 0.0f && chance <= 1.0f)) return fail(c, LP_ERR_INVALID, "lp_set_params: chance %g", chance);
+    if (!(w_threshold >= 0.0f) || !(factor > 0.0f)) return fail(c, LP_ERR_INVALID, "lp_set_params: bad threshold/factor");
+    c->chance = chance;
+    c->w_th = w_threshold;
+    c->factor = factor;
+    c->seed = seed;
+    c->compat = compat & LP_COMPAT_ALL;
+    return LP_OK;
+}
+
+int lp_set_extra_tallies(lp_ctx *c, const int32_t *vox_n, const float *vox_d, int32_t n_rbins, float rbin_dr,
+                         int32_t n_det, const float *det_r)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_extra_tallies: ctx is NULL");
+    if (n_det < 0 || n_det > lp::kMaxDet) return fail(c, LP_ERR_RANGE, "lp_set_extra_tallies: %d rings > %d", n_det, lp::kMaxDet);
+    if (vox_n && vox_n[0] > 0) {
+        if (!vox_d || vox_n[1] <= 0 || vox_n[2] <= 0 || !(vox_d[0] > 0) || !(vox_d[1] > 0) || !(vox_d[2] > 0))
+            return fail(c, LP_ERR_INVALID, "lp_set_extra_tallies: bad voxel grid");
+        if ((int64_t)vox_n[0] * vox_n[1] * vox_n[2] > (int64_t(1) << 31))
+            return fail(c, LP_ERR_RANGE, "lp_set_extra_tallies: voxel grid too large");
+        std::memcpy(c->vox_n, vox_n, 12);
+        std::memcpy(c->vox_d, vox_d, 12);
+    } else {
+        c->vox_n[0] = c->vox_n[1] = c->vox_n[2] = 0;
+    }
+    if (n_rbins < 0 || (n_rbins > 0 && !(rbin_dr > 0))) return fail(c, LP_ERR_INVALID, "lp_set_extra_tallies: bad radial bins");
+    c->n_rbins = n_rbins;
+    c->rbin_dr = rbin_dr;
+    c->det_r.assign(det_r ? det_r : (const float *)nullptr, det_r ? det_r + 2 * n_det : (const float *)nullptr);
+    c->tally_dirty = true;
+    return LP_OK;
+}
+
+int lp_set_max_steps(lp_ctx *c, int64_t max_steps)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_max_steps: ctx is NULL");
+    c->max_steps = max_steps;
+    return LP_OK;
+}
+
+int lp_set_exit_records(lp_ctx *c, int64_t capacity)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_exit_records: ctx is NULL");
+    if (capacity < 0 || capacity > (int64_t(1) << 30)) return fail(c, LP_ERR_RANGE, "lp_set_exit_records: capacity");
+    c->exit_cap = capacity;
+    return LP_OK;
+}
+
+int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_run: ctx is NULL");
+    if (n < 0 || first < 0) return fail(c, LP_ERR_INVALID, "lp_run: negative photon range");
+    c->h2d_bytes = 0;
+    int r = upload(c);
+    if (r) return r;
+    if (n == 0) return LP_OK;
+    int nodes_smem, tris_smem;
+    smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
+    const int smem = lp::smem_bytes(c->n_media, nodes_smem, tris_smem);
+    int per_sm = 0;
+    LP_CUDA(c, lp::transport_occupancy(smem, &per_sm));
+    if (per_sm < 1) return fail(c, LP_ERR_CUDA, "lp_run: transport kernel does not fit on an SM");
+    KParams P;
+    fill_params(c, P, first, n, nodes_smem, tris_smem);
+    LP_CUDA(c, cudaMemsetAsync(c->work.p, 0, 8, c->stream));
+    if (c->exit_cap > 0) LP_CUDA(c, cudaMemsetAsync(c->exit_rec.p, 0, (size_t)c->exit_cap * 32, c->stream));
+    LP_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    c->h2d_bytes += (int64_t)sizeof(KParams);
+    c->st_nodes_smem = nodes_smem;
+    c->st_tris_smem = tris_smem;
+    c->st_smem = smem;
+    c->st_per_sm = per_sm;
+    c->st_grid = c->num_sms * per_sm;
+    LP_CUDA(c, lp::launch_transport(P, c->num_sms * per_sm, smem, c->stream));
+    LP_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->launched = true;
+    return LP_OK;
+}
+
+int lp_sync(lp_ctx *c)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_sync: ctx is NULL");
+    LP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->launched) {
+        LP_CUDA(c, cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+        c->launched = false;
+    }
+    return LP_OK;
+}
+
+int lp_run(lp_ctx *c, int64_t first, int64_t n)
+{
+    int r = lp_run_async(c, first, n);
+    if (r) return r;
+    return lp_sync(c);
+}
+
+int lp_zero_tallies(lp_ctx *c)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_zero_tallies: ctx is NULL");
+    if (c->tally_dirty) return LP_OK;  // reallocated and zeroed on the next run
+    int r = zero_tallies(c);
+    if (r) return r;
+    LP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LP_OK;
+}
+
+int lp_get_geometry(lp_ctx *c, lp_geometry *out)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_geometry: NULL argument");
+    if (!c->have_grid) return fail(c, LP_ERR_STATE, "lp_get_geometry: tally grid not set");
+    *out = c->geo;
+    return LP_OK;
+}
+
+int lp_get_tallies(lp_ctx *c, lp_tallies *out)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_tallies: NULL argument");
+    if (c->tally_dirty || !c->sft.p) return fail(c, LP_ERR_STATE, "lp_get_tallies: nothing has run");
+    const lp_geometry &g = c->geo;
+    c->h_sft.resize((size_t)g.sft_nx * g.sft_ny * 3);
+    c->h_rtd.resize((size_t)g.dimR * g.dimAlpha * 3);
+    c->h_rz.resize((size_t)g.rz_nr * g.rz_nz * 2);
+    c->h_vox.resize((size_t)n_vox(c));
+    c->h_rbins.resize((size_t)c->n_rbins * 2);
+    c->h_region.resize((size_t)c->n_media);
+    c->h_det.resize(c->det_r.size());
+    cudaStream_t s = c->stream;
+    LP_CUDA(c, cudaMemcpyAsync(c->h_sft.data(), c->sft.p, c->h_sft.size() * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->h_rtd.data(), c->rtd.p, c->h_rtd.size() * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->h_rz.data(), c->rz.p, c->h_rz.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!c->h_vox.empty())
+        LP_CUDA(c, cudaMemcpyAsync(c->h_vox.data(), c->vox.p, c->h_vox.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!c->h_rbins.empty())
+        LP_CUDA(c, cudaMemcpyAsync(c->h_rbins.data(), c->rbins.p, c->h_rbins.size() * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->h_region.data(), c->region.p, c->h_region.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!c->h_det.empty())
+        LP_CUDA(c, cudaMemcpyAsync(c->h_det.data(), c->det.p, c->h_det.size() * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaMemcpyAsync(out->counters, c->counters.p, LP_NCOUNTERS * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaStreamSynchronize(s));
+    c->d2h_bytes = (int64_t)(c->h_sft.size() + c->h_rtd.size() + c->h_rz.size() + c->h_vox.size() +
+                             c->h_rbins.size() + c->h_region.size() + c->h_det.size() + LP_NCOUNTERS) * 8;
+    out->sft = c->h_sft.data();
+    out->rtd = c->h_rtd.data();
+    out->rz = c->h_rz.data();
+    out->vox = c->h_vox.data();
+    out->rbins = c->h_rbins.data();
+    out->region = c->h_region.data();
+    out->det = c->h_det.data();
+    out->n_vox = (int64_t)c->h_vox.size();
+    out->n_rbins = c->n_rbins;
+    out->n_region = c->n_media;
+    out->n_det = (int64_t)c->det_r.size() / 2;
+    return LP_OK;
+}
+
+int lp_get_exit_records(lp_ctx *c, float *out, int64_t n)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_exit_records: NULL argument");
+    if (n < 0 || n > c->exit_cap) return fail(c, LP_ERR_RANGE, "lp_get_exit_records: %lld > capacity", (long long)n);
+    if (n == 0) return LP_OK;
+    LP_CUDA(c, cudaMemcpyAsync(out, c->exit_rec.p, (size_t)n * 32, cudaMemcpyDeviceToHost, c->stream));
+    LP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LP_OK;
+}
+
+int lp_get_stats(lp_ctx *c, lp_stats *out)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_stats: NULL argument");
+    std::memset(out, 0, sizeof *out);
+    out->n_tri = c->n_tri;
+    out->n_nodes = (int64_t)c->bvh.node_a.size();
+    out->bvh_depth = c->bvh.depth;
+    out->nodes_smem = c->st_nodes_smem;
+    out->tris_smem = c->st_tris_smem;
+    out->smem_bytes = c->st_smem;
+    out->blocks_per_sm = c->st_per_sm;
+    out->grid = c->st_grid;
+    out->block = lp::block_size();
+    out->num_sms = c->num_sms;
+    out->h2d_bytes = c->h2d_bytes;
+    out->d2h_bytes = c->d2h_bytes;
+    out->last_kernel_ms = c->last_ms;
+    return LP_OK;
+}
+
+int lp_get_device_tallies(lp_ctx *c, lp_device_tallies *out)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_device_tallies: NULL argument");
+    if (c->tally_dirty || !c->sft.p) return fail(c, LP_ERR_STATE, "lp_get_device_tallies: tallies not allocated yet");
+    const lp_geometry &g = c->geo;
+    out->sft = (uint64_t *)c->sft.p;
+    out->rtd = (uint64_t *)c->rtd.p;
+    out->rz = (uint64_t *)c->rz.p;
+    out->vox = (uint64_t *)c->vox.p;
+    out->rbins = (uint64_t *)c->rbins.p;
+    out->region = (uint64_t *)c->region.p;
+    out->det = (uint64_t *)c->det.p;
+    out->counters = (uint64_t *)c->counters.p;
+    out->n_sft = (int64_t)g.sft_nx * g.sft_ny * 3;
+    out->n_rtd = (int64_t)g.dimR * g.dimAlpha * 3;
+    out->n_rz = (int64_t)g.rz_nr * g.rz_nz * 2;
+    out->n_vox = n_vox(c);
+    out->n_rbins = (int64_t)c->n_rbins * 2;
+    out->n_region = c->n_media;
+    out->n_det = (int64_t)c->det_r.size();
+    out->n_counters = LP_NCOUNTERS;
+    out->stream = (void *)c->stream;
+    return LP_OK;
+}
+
+int lp_fp32_peak(int device, double *tflops)
+{
+    if (!tflops) return fail(nullptr, LP_ERR_INVALID, "lp_fp32_peak: NULL argument");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_fp32_peak");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    *tflops = lp::fma_peak_tflops(sms);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_fp32_peak");
+    return LP_OK;
+}
+
+int lp_last_kernel_ms(lp_ctx *c, float *ms)
+{
+    if (!c || !ms) return fail(c, LP_ERR_INVALID, "lp_last_kernel_ms: NULL argument");
+    *ms = c->last_ms;
+    return LP_OK;
+}
+
+int lp_query_triangles(lp_ctx *c, int64_t n, const float *orig, const float *dir, const int32_t *ref_tri,
+                       const float *t_max, int32_t *id_out, float *t_out)
+{
+    if (!c || !orig || !dir || !ref_tri || !t_max || !id_out || !t_out)
+        return fail(c, LP_ERR_INVALID, "lp_query_triangles: NULL argument");
+    if (!c->have_mesh) return fail(c, LP_ERR_STATE, "lp_query_triangles: no mesh");
+    if (n <= 0) return LP_OK;
+    LP_CUDA(c, cudaSetDevice(c->device));
+    int ur = upload_mesh(c);
+    if (ur) return ur;
+    DevBuf<float> o, d, tm, to;
+    DevBuf<int32_t> rf, io;
+    LP_CUDA(c, o.ensure((size_t)n * 3));
+    LP_CUDA(c, d.ensure((size_t)n * 3));
+    LP_CUDA(c, tm.ensure((size_t)n));
+    LP_CUDA(c, to.ensure((size_t)n));
+    LP_CUDA(c, rf.ensure((size_t)n));
+    LP_CUDA(c, io.ensure((size_t)n));
+    cudaStream_t s = c->stream;
+    LP_CUDA(c, cudaMemcpyAsync(o.p, orig, (size_t)n * 12, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(d.p, dir, (size_t)n * 12, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(tm.p, t_max, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(rf.p, ref_tri, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    int nodes_smem, tris_smem;
+    smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
+    KParams P;
+    fill_params(c, P, 0, 0, nodes_smem, tris_smem);
+    const int smem = lp::smem_bytes(c->n_media, nodes_smem, tris_smem);
+    LP_CUDA(c, lp::launch_query(P, smem, n, o.p, d.p, rf.p, tm.p, io.p, to.p, s));
+    LP_CUDA(c, cudaMemcpyAsync(id_out, io.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaMemcpyAsync(t_out, to.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaStreamSynchronize(s));
+    o.release(); d.release(); tm.release(); to.release(); rf.release(); io.release();
+    return LP_OK;
+}
+
+int lp_philox_blocks(int device, const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out)
+{
+    if (!ctr || !key || !out || n < 0) return fail(nullptr, LP_ERR_INVALID, "lp_philox_blocks: bad argument");
+    if (n == 0) return LP_OK;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_philox_blocks");
+    DevBuf<uint32_t> b;
+    if ((e = b.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(nullptr, e, "lp_philox_blocks: alloc");
+    e = lp::launch_philox(ctr, key, n, b.p, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, b.p, (size_t)n * 16, cudaMemcpyDeviceToHost);
+    b.release();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_philox_blocks");
+    return LP_OK;
+}
+
+}  // extern "C"

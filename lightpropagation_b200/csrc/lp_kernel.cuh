@@ -1,0 +1,265 @@
+// lp_kernel.cuh -- device-side data layout and helpers of the transport kernel.
+//
+// Arithmetic follows src/Simulation/MCLightPropagation.cl operation by operation
+// (same operand order, IEEE division and square root, no contraction: the file is
+// compiled with --fmad=false), so a photon that consumes the same random numbers
+// follows the same trajectory as in the reference kernel up to the last-place
+// differences of logf/cosf/acosf.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lp {
+
+constexpr int kMaxMedia = 64;
+constexpr int kMaxDet = 32;
+constexpr int kStackDepth = 64;
+constexpr float kNoHit = 10000.0f;   // FindTriangleInPath's initial distance (.cl:1042)
+
+struct Medium {
+    float n, mua, mus, g;
+    float mut;      // mua + mus
+    float alb;      // mua / (mua + mus)
+    int32_t absorbs;  // mua > 0 && mus > 0  (Absorb, .cl:841-847)
+    int32_t ambient;  // mua == 0 && mus == 0 (step = distance to boundary, .cl:1405-1410)
+};
+
+struct KParams {
+    // mesh (see lp_bvh.hpp)
+    const float4 *node_a, *node_b, *node_c;
+    const int4 *node_d;
+    const float4 *tri_a, *tri_b, *tri_c;
+    const float4 *tri_attr;   // by original index: unit normal, (inner | outer << 16) bits
+    int32_t n_nodes, n_tri, nodes_smem, tris_smem;
+    // media
+    const Medium *media;
+    int32_t n_media;
+    // source and frame
+    float p0x, p0y, p0z, v0x, v0y, v0z;
+    float poix, poiy, poiz;
+    float ezx, ezy, ezz;             // eZ as given (sign test of the axis override)
+    float nxx, nxy, nxz, nyx, nyy, nyz, nzx, nzy, nzz;  // normalised eX, eY, eZ
+    float Rsp, distMin, exitScale, w0;
+    // run parameters
+    float chance, w_th, factor;
+    int32_t fetal_id;
+    uint32_t compat;
+    uint32_t key0, key1, stream;
+    int64_t first, n, max_steps;
+    // reference tally layout
+    int32_t hx, hy, sft_nx, dimR, dimAlpha, rz_nr, rz_nz;
+    float dg[6];
+    // tallies (fixed point, 2^32 per unit weight)
+    unsigned long long *sft, *rtd, *rz, *vox, *rbins, *region, *det, *counters;
+    int32_t vox_nx, vox_ny, vox_nz;
+    float vox_dx, vox_dy, vox_dz;
+    int32_t n_rbins;
+    float rbin_dr;
+    int32_t n_det;
+    float det_lo[kMaxDet], det_hi[kMaxDet];
+    float *exit_rec;
+    int64_t exit_cap;
+    // scratch: photon work counter
+    unsigned long long *work;
+};
+
+// ----------------------------------------------------------------- Philox4x32-10
+__device__ __forceinline__ void philox4x32_10(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t &c3,
+                                              uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Per-photon stream: counter (photon lo, photon hi, block, stream), key = seed.
+struct Rng {
+    uint32_t plo, phi, blk, used;
+    uint32_t b0, b1, b2, b3;
+    __device__ __forceinline__ void start(uint64_t pid)
+    {
+        plo = (uint32_t)pid;
+        phi = (uint32_t)(pid >> 32);
+        blk = 0;
+        used = 4;
+    }
+    __device__ __forceinline__ float next(uint32_t k0, uint32_t k1, uint32_t stream)
+    {
+        if (used == 4) {
+            b0 = plo; b1 = phi; b2 = blk; b3 = stream;
+            philox4x32_10(b0, b1, b2, b3, k0, k1);
+            ++blk;
+            used = 0;
+        }
+        const uint32_t x = b0;
+        b0 = b1; b1 = b2; b2 = b3;
+        ++used;
+        return __uint2float_rn(x >> 8) * 0x1.0p-24f;
+    }
+};
+
+// ------------------------------------------------------------- small vectors
+struct V3 { float x, y, z; };
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross3(V3 a, V3 b)
+{
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ V3 scl3(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+// normalize(): v / |v|, zero vector unchanged (OpenCL semantics)
+__device__ __forceinline__ V3 norm3(V3 v)
+{
+    const float l = sqrtf(dot3(v, v));
+    if (l == 0.0f) return v;
+    return v3(v.x / l, v.y / l, v.z / l);
+}
+__device__ __forceinline__ float sign_cl(float x)
+{
+    if (x > 0.0f) return 1.0f;
+    if (x < 0.0f) return -1.0f;
+    if (x != x) return 0.0f;
+    return x;
+}
+__device__ __forceinline__ unsigned long long fix32(float w)
+{
+    return (w > 0.0f) ? __float2ull_rn(w * 4294967296.0f) : 0ull;
+}
+__device__ __forceinline__ int trunc_sat(float q)
+{
+    if (q != q) return 0;
+    if (q > 1e9f) return 1000000000;
+    if (q < -1e9f) return -1000000000;
+    return (int)q;
+}
+__device__ __forceinline__ int trunc_sat_d(double q)
+{
+    if (q != q) return 0;
+    if (q > 1e9) return 1000000000;
+    if (q < -1e9) return -1000000000;
+    return (int)q;
+}
+
+// ------------------------------------------------------------- BVH query
+// Nearest triangle along (p, v) with t in (0, bound] and t < 10000, excluding
+// ref_tri; equal distances resolve to the lower original index.  Returns the
+// original index or -1; *t_out = distance or 10000.
+struct MeshView {
+    const float4 *na, *nb, *nc;
+    const int4 *nd;
+    const float4 *ta, *tb, *tc;
+    const float4 *s_na, *s_nb, *s_nc;
+    const int4 *s_nd;
+    const float4 *s_ta, *s_tb, *s_tc;
+    int32_t nodes_smem, tris_smem;
+};
+
+__device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, int ref_tri, float &best,
+                                         int &bid)
+{
+    float4 a, b, c;
+    if (j < M.tris_smem) {
+        a = M.s_ta[j]; b = M.s_tb[j]; c = M.s_tc[j];
+    } else {
+        a = __ldg(M.ta + j); b = __ldg(M.tb + j); c = __ldg(M.tc + j);
+    }
+    const int o = __float_as_int(c.y);
+    if (o == ref_tri) return;
+    const V3 Mv = v3(a.x, a.y, a.z), E = v3(a.w, b.x, b.y), F = v3(b.z, b.w, c.x);
+    const V3 G = sub3(p, Mv);
+    const V3 GE = cross3(G, E), VF = cross3(v, F);
+    float t = dot3(GE, F);
+    const float w = dot3(VF, E);
+    float k = dot3(VF, G);
+    float l = dot3(GE, v);
+    t = t / w;
+    k = k / w;
+    l = l / w;
+    if (t > 0.0f && t < kNoHit && k >= 0.0f && l >= 0.0f && (k + l) < 1.0f &&
+        (t < best || (t == best && o < bid))) {
+        best = t;
+        bid = o;
+    }
+}
+
+__device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
+                                             float &t_out)
+{
+    float best = fminf(bound, kNoHit);
+    int bid = 0x7fffffff;
+    const float ix = 1.0f / (fabsf(v.x) > 1e-30f ? v.x : copysignf(1e-30f, v.x));
+    const float iy = 1.0f / (fabsf(v.y) > 1e-30f ? v.y : copysignf(1e-30f, v.y));
+    const float iz = 1.0f / (fabsf(v.z) > 1e-30f ? v.z : copysignf(1e-30f, v.z));
+    const float ox = p.x * ix, oy = p.y * iy, oz = p.z * iz;
+    int stack[kStackDepth];
+    int sp = 0;
+    int node = 0;
+    for (;;) {
+        float4 a, b, c;
+        int4 d;
+        if (node < M.nodes_smem) {
+            a = M.s_na[node]; b = M.s_nb[node]; c = M.s_nc[node]; d = M.s_nd[node];
+        } else {
+            a = __ldg(M.na + node); b = __ldg(M.nb + node); c = __ldg(M.nc + node); d = __ldg(M.nd + node);
+        }
+        // slab tests of both children against [0, best]
+        float t0, t1, tn0, tf0, tn1, tf1;
+        t0 = a.x * ix - ox; t1 = a.y * ix - ox;
+        tn0 = fminf(t0, t1); tf0 = fmaxf(t0, t1);
+        t0 = a.z * iy - oy; t1 = a.w * iy - oy;
+        tn0 = fmaxf(tn0, fminf(t0, t1)); tf0 = fminf(tf0, fmaxf(t0, t1));
+        t0 = c.x * iz - oz; t1 = c.y * iz - oz;
+        tn0 = fmaxf(tn0, fminf(t0, t1)); tf0 = fminf(tf0, fmaxf(t0, t1));
+        t0 = b.x * ix - ox; t1 = b.y * ix - ox;
+        tn1 = fminf(t0, t1); tf1 = fmaxf(t0, t1);
+        t0 = b.z * iy - oy; t1 = b.w * iy - oy;
+        tn1 = fmaxf(tn1, fminf(t0, t1)); tf1 = fminf(tf1, fmaxf(t0, t1));
+        t0 = c.z * iz - oz; t1 = c.w * iz - oz;
+        tn1 = fmaxf(tn1, fminf(t0, t1)); tf1 = fminf(tf1, fmaxf(t0, t1));
+        // widen the far end relative to best so rounding never culls a tie
+        const float lim = best * 1.000001f + 1e-6f;
+        bool h0 = fmaxf(tn0, 0.0f) <= fminf(tf0, lim);
+        bool h1 = fmaxf(tn1, 0.0f) <= fminf(tf1, lim);
+        if (h0 && d.x < 0) {
+            const int e = ~d.x, f = e >> 3, cnt = (e & 7) + 1;
+            for (int j = f; j < f + cnt; ++j) test_tri(M, j, p, v, ref_tri, best, bid);
+            h0 = false;
+        }
+        if (h1 && d.y < 0) {
+            const int e = ~d.y, f = e >> 3, cnt = (e & 7) + 1;
+            for (int j = f; j < f + cnt; ++j) test_tri(M, j, p, v, ref_tri, best, bid);
+            h1 = false;
+        }
+        if (h0 && h1) {
+            const bool first0 = tn0 <= tn1;
+            if (sp < kStackDepth) stack[sp++] = first0 ? d.y : d.x;
+            node = first0 ? d.x : d.y;
+        } else if (h0) {
+            node = d.x;
+        } else if (h1) {
+            node = d.y;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    if (bid == 0x7fffffff) {
+        t_out = kNoHit;
+        return -1;
+    }
+    t_out = best;
+    return bid;
+}
+
+}  // namespace lp

@@ -23,7 +23,7 @@
 
 namespace clref {
 
-extern long g_global_id;
+extern thread_local long g_global_id;
 extern long g_global_size;
 
 typedef int event_t;

@@ -7,6 +7,7 @@
  * The resulting library is the pin for lp_oracle.c; it is never shipped.
  */
 #include "clshim.hpp"
+#include <thread>
 #include <vector>
 
 #define __kernel
@@ -17,7 +18,7 @@
 #define global
 
 namespace clref {
-long g_global_id = 0;
+thread_local long g_global_id = 0;
 long g_global_size = 1;
 #include LP_CL_SOURCE
 } // namespace clref
@@ -70,6 +71,43 @@ int clref_run(int numTriangles, float factor, const float *vStart, const int *vS
                                   dimsXYZ, e_P0XYZ, gridDims, triangles, normals, mediumIDs,
                                   nMuasG, rand3Arr, inxtInxtpLocked);
     }
+    return 0;
+}
+
+/* CPU baseline driver: n_items work-items over nthreads host threads.  Each thread
+ * plays one OpenCL work-group of the reference: it starts from the same copy of the
+ * ran3 table (every work-group of a launch does, MCLightPropagation.cl:1316-1317),
+ * runs its work-items one after another and writes its exit records; each thread
+ * has its own r-z buffer (rz_cells floats x3 each, caller-allocated nthreads times).
+ * Returns 0. */
+int clref_run_mt(int numTriangles, float factor, const float *vStart, const int *vStartOcc,
+                 const float *pStart3, float chance, float w_threshold, int fetalTissueID,
+                 float *SurfFetalTransRxyG, float *rz_buffers, long rz_stride_cells, long rz_offset_cells,
+                 const float *dimsXYZ, const float *e_P0XYZ, const float *gridDims, float *triangles,
+                 float *normals, const int *mediumIDs, const float *nMuasG, const float *rand3Arr0,
+                 const int *inxt0, long n_items, int nthreads)
+{
+    clref::float3 pStart(pStart3[0], pStart3[1], pStart3[2]);
+    clref::g_global_size = n_items;
+    if (nthreads < 1) nthreads = 1;
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t) {
+        th.emplace_back([=]() {
+            float st[56];
+            int ix[3];
+            for (int i = 0; i < 56; ++i) st[i] = rand3Arr0[i];
+            for (int i = 0; i < 3; ++i) ix[i] = inxt0[i];
+            float *rz = rz_buffers + 3 * (rz_stride_cells * t + rz_offset_cells);
+            const long lo = n_items * t / nthreads, hi = n_items * (t + 1) / nthreads;
+            for (long i = lo; i < hi; ++i) {
+                clref::g_global_id = i;
+                clref::MCLightPropagation(numTriangles, factor, vStart, vStartOcc, pStart, chance,
+                                          w_threshold, fetalTissueID, SurfFetalTransRxyG, rz, dimsXYZ,
+                                          e_P0XYZ, gridDims, triangles, normals, mediumIDs, nMuasG, st, ix);
+            }
+        });
+    }
+    for (auto &x : th) x.join();
     return 0;
 }
 
