@@ -100,6 +100,12 @@ int lp_set_media(lp_ctx *ctx, int32_t n_media, const float *nmuasg);
  * 12 floats POI, eX, eY, eZ (the kernel's e_P0XYZ). */
 int lp_set_source(lp_ctx *ctx, const float *p_start, const float *v_start,
                   const int32_t *v_occ, int32_t k, const float *ep0xyz);
+/* Fibre source (no reference counterpart; the reference launches a pencil beam):
+ * start points uniform on a disk of `radius` around p_start in the (eX, eY) plane,
+ * directions uniform in solid angle within the cone of half-angle asin(na / n0)
+ * about eZ (n0 = refractive index of region 0).  radius = na = 0 restores the
+ * pencil beam. */
+int lp_set_fiber_source(lp_ctx *ctx, float radius, float na);
 /* SetDimensions + SetDetectionGridDimensions + SetFetalTissueID
  * (CalculatePropagation.cpp:536-539, 716-735, 792-794): model extent, detection
  * grid (x, y, z, r, phi, rho) and the fetal region id.  Fixes the image extents. */
@@ -114,6 +120,13 @@ int lp_set_params(lp_ctx *ctx, float chance, float w_threshold, float factor,
  * in the emitter frame, radial exit bins, ring detectors (n_det annuli r_lo, r_hi). */
 int lp_set_extra_tallies(lp_ctx *ctx, const int32_t *vox_n, const float *vox_d,
                          int32_t n_rbins, float rbin_dr, int32_t n_det, const float *det_r);
+/* Arithmetic of the transport kernel.  exact = 1 follows the reference kernel's
+ * floating-point operations one by one (same operand order, IEEE division, no FMA
+ * contraction), so with the same random numbers a photon retraces the CPU oracle's
+ * trajectory; exact = 0 (default) samples the same distributions with fewer
+ * operations (precomputed Henyey-Greenstein factors, direction-cosine scattering
+ * update, vector refraction, reciprocal multiplies, FMA). */
+int lp_set_arithmetic(lp_ctx *ctx, int exact);
 /* Per-photon step cap (watchdog); photons that reach it are stopped and counted. */
 int lp_set_max_steps(lp_ctx *ctx, int64_t max_steps);
 /* Keep the per-photon float8 exit records of the next runs (RecordFSTxy,

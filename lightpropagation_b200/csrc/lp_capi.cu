@@ -21,9 +21,11 @@
 #include "lp_kernel.cuh"
 
 namespace lp {
-int smem_bytes(int n_media, int nodes_smem, int tris_smem);
-cudaError_t launch_transport(const KParams &P, int grid, int smem, cudaStream_t s);
-cudaError_t transport_occupancy(int smem, int *blocks_per_sm);
+int smem_bytes(int nodes_smem, int tris_smem);
+cudaError_t launch_transport_fast(const KParams &P, int grid, int smem, cudaStream_t s);
+cudaError_t transport_occupancy_fast(int smem, int *blocks_per_sm);
+cudaError_t launch_transport_exact(const KParams &P, int grid, int smem, cudaStream_t s);
+cudaError_t transport_occupancy_exact(int smem, int *blocks_per_sm);
 cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *orig, const float *dir,
                          const int32_t *ref, const float *tmax, int32_t *id_out, float *t_out,
                          cudaStream_t s);
@@ -85,6 +87,7 @@ struct lp_ctx {
     float chance = 0.1f, w_th = 1e-4f, factor = 1.0f;
     uint64_t seed = 0x4C50;
     uint32_t compat = LP_COMPAT_ALL;
+    bool exact = false;   // reference-order arithmetic (lp_set_arithmetic)
     int64_t max_steps = 100000000;
     int32_t vox_n[3] = {0, 0, 0};
     float vox_d[3] = {1, 1, 1};
@@ -92,6 +95,7 @@ struct lp_ctx {
     float rbin_dr = 1.0f;
     std::vector<float> det_r;
     int64_t exit_cap = 0;
+    float fiber_radius = 0.0f, fiber_na = 0.0f;
     lp_geometry geo{};
     // device buffers
     DevBuf<float4> node_a, node_b, node_c, tri_a, tri_b, tri_c, attr;
@@ -236,6 +240,15 @@ int upload_media(lp_ctx *c)
         m[i].alb = q[1] / (q[1] + q[2]);
         m[i].absorbs = (q[1] > 0.0f && q[2] > 0.0f) ? 1 : 0;
         m[i].ambient = (q[1] == 0.0f && q[2] == 0.0f) ? 1 : 0;
+        m[i].inv_mut = (q[1] + q[2]) > 0.0f ? 1.0f / (q[1] + q[2]) : 0.0f;
+        m[i].inv_mua = q[1] > 0.0f ? 1.0f / q[1] : 0.0f;
+        const float g = q[3];
+        m[i].hg_a = 1.0f - g * g;
+        m[i].hg_b = 1.0f - g;
+        m[i].hg_c = 2.0f * g;
+        m[i].hg_d = 1.0f + g * g;
+        m[i].hg_inv2g = g != 0.0f ? 1.0f / (2.0f * g) : 0.0f;
+        m[i].pad_ = 0.0f;
     }
     LP_CUDA(c, c->media.ensure(lp::kMaxMedia));
     LP_CUDA(c, cudaMemcpyAsync(c->media.p, m.data(), m.size() * sizeof(Medium), cudaMemcpyHostToDevice,
@@ -326,6 +339,11 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.hx = g.dimx / 2; P.hy = g.dimy / 2; P.sft_nx = g.sft_nx;
     P.dimR = g.dimR; P.dimAlpha = g.dimAlpha; P.rz_nr = g.rz_nr; P.rz_nz = g.rz_nz;
     for (int i = 0; i < 6; ++i) P.dg[i] = c->det_grid[i];
+    P.inv_dr = 1.0f / c->det_grid[3];
+    P.inv_dz = 1.0f / c->det_grid[2];
+    P.inv_vdx = 1.0f / c->vox_d[0];
+    P.inv_vdy = 1.0f / c->vox_d[1];
+    P.inv_vdz = 1.0f / c->vox_d[2];
     P.sft = c->sft.p; P.rtd = c->rtd.p; P.rz = c->rz.p; P.vox = c->vox.p; P.rbins = c->rbins.p;
     P.region = c->region.p; P.det = c->det.p; P.counters = c->counters.p;
     P.vox_nx = c->vox_n[0]; P.vox_ny = c->vox_n[1]; P.vox_nz = c->vox_n[2];
@@ -337,6 +355,14 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
         P.det_lo[k] = c->det_r[2 * k];
         P.det_hi[k] = c->det_r[2 * k + 1];
     }
+    P.src_type = (c->fiber_radius > 0.0f || c->fiber_na > 0.0f) ? 1 : 0;
+    P.src_radius = c->fiber_radius;
+    {
+        // the query-only path runs without media: the cone is unused there
+        const float n0 = c->nmuasg.empty() ? 1.0f : c->nmuasg[0];
+        const float s = c->fiber_na / n0;
+        P.src_cos_max = s < 1.0f ? std::sqrt(1.0f - s * s) : 0.0f;
+    }
     P.exit_rec = c->exit_cap > 0 ? c->exit_rec.p : nullptr;
     P.exit_cap = c->exit_cap;
     P.work = c->work.p;
@@ -345,7 +371,7 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
 // shared-memory staging: as many top BVH levels and leading triangles as fit the budget
 void smem_plan(const lp_ctx *c, int budget, int &nodes_smem, int &tris_smem)
 {
-    const int base = lp::smem_bytes(c->n_media, 0, 0);
+    const int base = lp::smem_bytes(0, 0);
     int room = std::max(0, budget - base);
     const int nn = (int)c->bvh.node_a.size(), nt = (int)c->bvh.tri_a.size();
     nodes_smem = std::min(nn, room / 64);
@@ -461,6 +487,16 @@ int lp_set_source(lp_ctx *c, const float *p_start, const float *v_start, const i
     return LP_OK;
 }
 
+int lp_set_fiber_source(lp_ctx *c, float radius, float na)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_fiber_source: ctx is NULL");
+    if (!(radius >= 0.0f) || !(na >= 0.0f) || !(na < 1.0f))
+        return fail(c, LP_ERR_INVALID, "lp_set_fiber_source: radius %g, NA %g", radius, na);
+    c->fiber_radius = radius;
+    c->fiber_na = na;
+    return LP_OK;
+}
+
 int lp_set_tally_grid(lp_ctx *c, const float *dimensions, const float *det_grid, int32_t fetal_id)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_tally_grid: ctx is NULL");
@@ -517,6 +553,13 @@ int lp_set_extra_tallies(lp_ctx *c, const int32_t *vox_n, const float *vox_d, in
     return LP_OK;
 }
 
+int lp_set_arithmetic(lp_ctx *c, int exact)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_arithmetic: ctx is NULL");
+    c->exact = exact != 0;
+    return LP_OK;
+}
+
 int lp_set_max_steps(lp_ctx *c, int64_t max_steps)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_max_steps: ctx is NULL");
@@ -542,9 +585,9 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
     if (n == 0) return LP_OK;
     int nodes_smem, tris_smem;
     smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
-    const int smem = lp::smem_bytes(c->n_media, nodes_smem, tris_smem);
+    const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     int per_sm = 0;
-    LP_CUDA(c, lp::transport_occupancy(smem, &per_sm));
+    LP_CUDA(c, c->exact ? lp::transport_occupancy_exact(smem, &per_sm) : lp::transport_occupancy_fast(smem, &per_sm));
     if (per_sm < 1) return fail(c, LP_ERR_CUDA, "lp_run: transport kernel does not fit on an SM");
     KParams P;
     fill_params(c, P, first, n, nodes_smem, tris_smem);
@@ -557,7 +600,8 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
     c->st_smem = smem;
     c->st_per_sm = per_sm;
     c->st_grid = c->num_sms * per_sm;
-    LP_CUDA(c, lp::launch_transport(P, c->num_sms * per_sm, smem, c->stream));
+    LP_CUDA(c, c->exact ? lp::launch_transport_exact(P, c->num_sms * per_sm, smem, c->stream)
+                        : lp::launch_transport_fast(P, c->num_sms * per_sm, smem, c->stream));
     LP_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     c->launched = true;
     return LP_OK;
@@ -742,7 +786,7 @@ int lp_query_triangles(lp_ctx *c, int64_t n, const float *orig, const float *dir
     smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
     KParams P;
     fill_params(c, P, 0, 0, nodes_smem, tris_smem);
-    const int smem = lp::smem_bytes(c->n_media, nodes_smem, tris_smem);
+    const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     LP_CUDA(c, lp::launch_query(P, smem, n, o.p, d.p, rf.p, tm.p, io.p, to.p, s));
     LP_CUDA(c, cudaMemcpyAsync(id_out, io.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
     LP_CUDA(c, cudaMemcpyAsync(t_out, to.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));

@@ -22,6 +22,10 @@ struct Medium {
     float alb;      // mua / (mua + mus)
     int32_t absorbs;  // mua > 0 && mus > 0  (Absorb, .cl:841-847)
     int32_t ambient;  // mua == 0 && mus == 0 (step = distance to boundary, .cl:1405-1410)
+    // precomputed factors of the fast arithmetic mode
+    float inv_mut, inv_mua;
+    float hg_a, hg_b, hg_c, hg_d, hg_inv2g;   // 1-g^2, 1-g, 2g, 1+g^2, 1/(2g)
+    float pad_;
 };
 
 struct KParams {
@@ -40,6 +44,8 @@ struct KParams {
     float ezx, ezy, ezz;             // eZ as given (sign test of the axis override)
     float nxx, nxy, nxz, nyx, nyy, nyz, nzx, nzy, nzz;  // normalised eX, eY, eZ
     float Rsp, distMin, exitScale, w0;
+    int32_t src_type;                // 0 pencil beam (reference), 1 fibre disk + cone
+    float src_radius, src_cos_max;
     // run parameters
     float chance, w_th, factor;
     int32_t fetal_id;
@@ -49,6 +55,7 @@ struct KParams {
     // reference tally layout
     int32_t hx, hy, sft_nx, dimR, dimAlpha, rz_nr, rz_nz;
     float dg[6];
+    float inv_dr, inv_dz, inv_vdx, inv_vdy, inv_vdz;   // reciprocals for the fast mode
     // tallies (fixed point, 2^32 per unit weight)
     unsigned long long *sft, *rtd, *rz, *vox, *rbins, *region, *det, *counters;
     int32_t vox_nx, vox_ny, vox_nz;
@@ -81,29 +88,20 @@ __device__ __forceinline__ void philox4x32_10(uint32_t &c0, uint32_t &c1, uint32
     }
 }
 
-// Per-photon stream: counter (photon lo, photon hi, block, stream), key = seed.
-struct Rng {
-    uint32_t plo, phi, blk, used;
-    uint32_t b0, b1, b2, b3;
-    __device__ __forceinline__ void start(uint64_t pid)
+// One Philox block per event: counter (photon lo, photon hi, event, stream), key =
+// seed.  Event 0 samples the source, loop iteration i is event i + 1.  The four words
+// are the event's draw slots (step, Fresnel or polar angle, azimuth, roulette), each
+// mapped to ((x >> 8) | 1) * 2^-24, a uniform in (0, 1) that is never 0.
+struct EventRng {
+    float u0, u1, u2, u3;
+    __device__ __forceinline__ void draw(uint64_t pid, uint32_t event, uint32_t stream, uint32_t k0, uint32_t k1)
     {
-        plo = (uint32_t)pid;
-        phi = (uint32_t)(pid >> 32);
-        blk = 0;
-        used = 4;
-    }
-    __device__ __forceinline__ float next(uint32_t k0, uint32_t k1, uint32_t stream)
-    {
-        if (used == 4) {
-            b0 = plo; b1 = phi; b2 = blk; b3 = stream;
-            philox4x32_10(b0, b1, b2, b3, k0, k1);
-            ++blk;
-            used = 0;
-        }
-        const uint32_t x = b0;
-        b0 = b1; b1 = b2; b2 = b3;
-        ++used;
-        return __uint2float_rn(x >> 8) * 0x1.0p-24f;
+        uint32_t c0 = (uint32_t)pid, c1 = (uint32_t)(pid >> 32), c2 = event, c3 = stream;
+        philox4x32_10(c0, c1, c2, c3, k0, k1);
+        u0 = __uint2float_rn((c0 >> 8) | 1u) * 0x1.0p-24f;
+        u1 = __uint2float_rn((c1 >> 8) | 1u) * 0x1.0p-24f;
+        u2 = __uint2float_rn((c2 >> 8) | 1u) * 0x1.0p-24f;
+        u3 = __uint2float_rn((c3 >> 8) | 1u) * 0x1.0p-24f;
     }
 };
 
@@ -183,6 +181,13 @@ __device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, i
     const float w = dot3(VF, E);
     float k = dot3(VF, G);
     float l = dot3(GE, v);
+    // Division-free filter, looser than the exact test below: t, k, l must share the
+    // sign of w, |k| + |l| may not exceed |w| and |t| may not exceed best * |w| (each
+    // with a relative margin far above the rounding of the divided values).  Only
+    // candidates that pass pay for the three IEEE divisions of the reference test.
+    const float aw = fabsf(w);
+    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= 0.0f && l >= 0.0f) : (t < 0.0f && k <= 0.0f && l <= 0.0f);
+    if (!sgn || fabsf(k) + fabsf(l) > aw * 1.0001f || fabsf(t) > best * aw * 1.0001f) return;
     t = t / w;
     k = k / w;
     l = l / w;

@@ -1,0 +1,17 @@
+// lp_transport_fast.cu -- production instantiation of the transport kernel
+// (Exact = false, compiled with FMA contraction; see lp_transport_impl.cuh).
+#include "lp_transport_impl.cuh"
+
+namespace lp {
+
+cudaError_t launch_transport_fast(const KParams &P, int grid, int smem, cudaStream_t s)
+{
+    return launch_transport_t<false>(P, grid, smem, s);
+}
+
+cudaError_t transport_occupancy_fast(int smem, int *blocks_per_sm)
+{
+    return transport_occupancy_t<false>(smem, blocks_per_sm);
+}
+
+}  // namespace lp

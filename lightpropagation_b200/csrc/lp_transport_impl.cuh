@@ -1,20 +1,31 @@
-// lp_transport.cu -- persistent photon-transport kernel for sm_100a.
+// lp_transport_impl.cuh -- persistent photon-transport kernel for sm_100a.
 //
-// One CUDA thread carries one photon packet at a time, as one OpenCL work-item
-// does in the reference (src/Simulation/MCLightPropagation.cl:1262-1606).  The
-// grid is persistent: each warp refills the lanes whose photon has finished with
-// new photon ids taken from a global counter, one atomicAdd per warp refill, so
-// lanes stay busy until the photon budget is spent.  Photon i always consumes
-// the Philox stream (key = seed, counter = (i, block, stream)), so results do not
-// depend on which thread traced which photon.
+// One CUDA thread carries one photon packet at a time, as one OpenCL work-item does
+// in the reference (src/Simulation/MCLightPropagation.cl:1262-1606).  The grid is
+// persistent: each warp refills the lanes whose photon has finished with new photon
+// ids taken from a global counter, one atomicAdd per warp refill, so lanes stay busy
+// until the photon budget is spent.  Photon i draws its random numbers from Philox
+// blocks (key = seed, counter = (i, event, stream)), so results do not depend on
+// which thread traced which photon; every loop iteration computes exactly one block,
+// which keeps the warp converged on the RNG.
 //
 // Per loop iteration (MCLightPropagation.cl:1375-1575):
-//   step length (.cl:1405-1442) -> nearest triangle within the step through the
-//   BVH (replaces the O(T) FindTriangleInPath, .cl:1037-1093) -> boundary
+//   step length (.cl:1405-1442) -> nearest triangle within the step through the BVH
+//   (replaces the O(T) FindTriangleInPath, .cl:1037-1093) -> boundary
 //   (TransmitOrReflect, .cl:921-1018) or absorb + Henyey-Greenstein scatter +
 //   absorption tallies (.cl:1513-1537) -> roulette (.cl:1539-1545).
-// At the end of a photon the exit record (.cl:1583-1594) is binned on the device
-// into the reference's SFT and RTd images (CalculatePropagation.cpp:1553-1626).
+// At the end of a photon its exit record (.cl:1583-1594) is binned on the device into
+// the reference's SFT and RTd images (CalculatePropagation.cpp:1553-1626).
+//
+// Exact = true  keeps the reference's arithmetic operation by operation (compiled
+//               with --fmad=false): a photon follows the oracle's trajectory for the
+//               same random numbers up to last-place differences of logf/cosf/acosf.
+// Exact = false (production) computes the same physics with fewer operations:
+//               Henyey-Greenstein sampling with precomputed factors, the direction-
+//               cosine update of Wang et al. (MCML, 1995) instead of two Rodrigues
+//               rotations (same distribution: polar angle from HG, uniform azimuth),
+//               vector refraction/reflection, reciprocal multiplies, FMA contraction.
+#pragma once
 #include <algorithm>
 
 #include "lp_kernel.cuh"
@@ -27,31 +38,39 @@ struct Photon {
     float px, py, pz, vx, vy, vz;
     float w, unfin, absorbed;
     float nvx, nvy, nvz;     // last boundary normal (CalcAlphaOut, .cl:1583)
-    float sft_s, sft_f, sft_t;
+    float exit_w;            // exit weight once scored
     int32_t curr, refTri;
-    bool fetal, roulette;
     uint32_t steps;
+    uint32_t flags;          // bit0 traversedFetalTissue, bit1 roulette, bits 2-3 exit kind
     unsigned long long region_acc;
     int64_t pid;
 };
+enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2 };
+enum : uint32_t { EXIT_NONE = 0, EXIT_SURF = 1, EXIT_SURF_FETAL = 2, EXIT_TRANS = 3 };
 
 struct Counters {
-    uint32_t scatter, boundary, query, roulette, miss, capped, rz_drop, vox_drop, photons, draws;
+    uint32_t scatter, boundary, query, roulette, rz_drop, vox_drop;
 };
 
-__device__ __forceinline__ float hg_cos_theta(float g, float xi)
+template <bool Exact>
+__device__ __forceinline__ float hg_cos_theta(const Medium &m, float xi)
 {
-    // VScatter (.cl:625-634)
-    float cosTheta = 0.0f;
-    const float g1 = (1.0f - g * g) / (1.0f - g + 2.0f * g * xi);
-    if (g != 0.0f) {
-        cosTheta = (1.0f + g * g - g1 * g1) / (2.0f * g);
-        if (cosTheta < -1.0f) cosTheta = -1.0f;
-        else if (cosTheta > 1.0f) cosTheta = 1.0f;
+    float cosTheta;
+    if (Exact) {
+        // VScatter (.cl:625-634)
+        const float g = m.g;
+        const float g1 = (1.0f - g * g) / (1.0f - g + 2.0f * g * xi);
+        if (g != 0.0f) cosTheta = (1.0f + g * g - g1 * g1) / (2.0f * g);
+        else cosTheta = 2.0f * xi - 1.0f;
     } else {
-        cosTheta = 2.0f * xi - 1.0f;
+        if (m.g != 0.0f) {
+            const float g1 = __fdividef(m.hg_a, m.hg_b + m.hg_c * xi);
+            cosTheta = (m.hg_d - g1 * g1) * m.hg_inv2g;
+        } else {
+            cosTheta = 2.0f * xi - 1.0f;
+        }
     }
-    return cosTheta;
+    return fminf(fmaxf(cosTheta, -1.0f), 1.0f);
 }
 
 // Rotate (.cl:697-708)
@@ -63,28 +82,55 @@ __device__ __forceinline__ V3 rotate(V3 vec, V3 axis, float c, float s)
     return add3(add3(scl3(nDx, axis), scl3(c, nXxXn)), scl3(s, nXx));
 }
 
-// VScatter (.cl:597-655)
-__device__ __forceinline__ V3 vscatter(V3 v, float g, float xt, float xp)
+__device__ __forceinline__ V3 fast_norm(V3 v)
 {
-    V3 e_rot = v3(0.0f, 0.0f, 0.0f);
-    if (v.z != 0.0f) {
-        const float z = -(v.x + v.y) / (v.z);
-        e_rot = v3(1.0f, 1.0f, z);
-    } else if (v.y != 0.0f) {
-        const float y = -(v.x) / (v.y);
-        e_rot = v3(1.0f, y, 0.0f);
-    } else if (v.x != 0.0f) {
-        e_rot = v3(0.0f, 1.0f, 0.0f);
+    const float r = rsqrtf(dot3(v, v));
+    return v3(v.x * r, v.y * r, v.z * r);
+}
+
+template <bool Exact>
+__device__ __forceinline__ V3 scatter_direction(V3 v, const Medium &m, float xt, float xp)
+{
+    const float cosTheta = hg_cos_theta<Exact>(m, xt);
+    if (Exact) {
+        // VScatter (.cl:597-655): rotate by theta about e_rot _|_ v, then by psi about v
+        V3 e_rot = v3(0.0f, 0.0f, 0.0f);
+        if (v.z != 0.0f) {
+            const float z = -(v.x + v.y) / (v.z);
+            e_rot = v3(1.0f, 1.0f, z);
+        } else if (v.y != 0.0f) {
+            const float y = -(v.x) / (v.y);
+            e_rot = v3(1.0f, y, 0.0f);
+        } else if (v.x != 0.0f) {
+            e_rot = v3(0.0f, 1.0f, 0.0f);
+        }
+        e_rot = norm3(e_rot);
+        const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
+        const float psi = 2.0f * 3.14159265358979323846f * xp;
+        const float cosPsi = cosf(psi);
+        float sinPsi = sqrtf(1.0f - cosPsi * cosPsi);
+        if (psi > 3.14159265358979323846f) sinPsi *= -1.0f;
+        const V3 rot_theta = norm3(rotate(v, e_rot, cosTheta, sinTheta));
+        return norm3(rotate(rot_theta, v, cosPsi, sinPsi));
+    } else {
+        // direction-cosine update (Wang, Jacques & Zheng, MCML 1995)
+        const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+        float sinPsi, cosPsi;
+        sincospif(2.0f * xp, &sinPsi, &cosPsi);
+        V3 r;
+        const float uz2 = 1.0f - v.z * v.z;
+        if (uz2 < 1e-10f) {
+            r = v3(sinTheta * cosPsi, sinTheta * sinPsi, copysignf(cosTheta, v.z));
+        } else {
+            const float it = rsqrtf(uz2);
+            const float temp = uz2 * it;  // sqrt(1 - uz^2)
+            const float st = sinTheta * it;
+            r = v3(st * (v.x * v.z * cosPsi - v.y * sinPsi) + v.x * cosTheta,
+                   st * (v.y * v.z * cosPsi + v.x * sinPsi) + v.y * cosTheta,
+                   -sinTheta * cosPsi * temp + v.z * cosTheta);
+        }
+        return fast_norm(r);
     }
-    e_rot = norm3(e_rot);
-    const float cosTheta = hg_cos_theta(g, xt);
-    const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
-    const float psi = 2.0f * 3.14159265358979323846f * xp;
-    const float cosPsi = cosf(psi);
-    float sinPsi = sqrtf(1.0f - cosPsi * cosPsi);
-    if (psi > 3.14159265358979323846f) sinPsi *= -1.0f;
-    const V3 rot_theta = norm3(rotate(v, e_rot, cosTheta, sinTheta));
-    return norm3(rotate(rot_theta, v, cosPsi, sinPsi));
 }
 
 // GetFresnel (.cl:857-907)
@@ -122,7 +168,7 @@ __device__ __forceinline__ void add_fix(unsigned long long *a, float w)
 }
 
 // Exit record binning of CalculatePropagation.cpp:1553-1626 plus radial bins and rings.
-__device__ void finish_photon(const KParams &P, const Photon &ph, Counters &cnt)
+static __device__ __noinline__ void finish_photon(const KParams &P, const Photon &ph)
 {
     const V3 v = v3(ph.vx, ph.vy, ph.vz), nv = v3(ph.nvx, ph.nvy, ph.nvz);
     const float alpha = fabsf(acosf(dot3(v, nv)));
@@ -132,15 +178,17 @@ __device__ void finish_photon(const KParams &P, const Photon &ph, Counters &cnt)
     const float cx = dot3(v3(P.nxx, P.nxy, P.nxz), pr);
     const float cy = dot3(v3(P.nyx, P.nyy, P.nyz), pr);
     const float cz = dot3(v3(P.nzx, P.nzy, P.nzz), pr);
+    const uint32_t kind = (ph.flags >> EXIT_SHIFT) & 3u;
+    const float s = (kind == EXIT_SURF || kind == EXIT_SURF_FETAL) ? ph.exit_w : 0.0f;
+    const float f = (kind == EXIT_SURF_FETAL) ? ph.exit_w : 0.0f;
+    const float t = (kind == EXIT_TRANS) ? ph.exit_w : 0.0f;
     const int64_t slot = ph.pid - P.first;
     if (P.exit_rec && slot >= 0 && slot < P.exit_cap) {
         float4 *r = reinterpret_cast<float4 *>(P.exit_rec + 8 * slot);
-        r[0] = make_float4(cx, cy, cz, ph.sft_s);
-        r[1] = make_float4(ph.sft_f, ph.sft_t, alpha, radius);
+        r[0] = make_float4(cx, cy, cz, s);
+        r[1] = make_float4(f, t, alpha, radius);
     }
-    cnt.photons++;
-    const float s = ph.sft_s, f = ph.sft_f, t = ph.sft_t;
-    if (s == 0.0f && f == 0.0f && t == 0.0f) return;
+    if (kind == EXIT_NONE) return;
     int x = trunc_sat(cx / P.dg[0]);
     int y = trunc_sat(cy / P.dg[1]);
     y = min(max(y, -P.hy), P.hy);
@@ -177,43 +225,58 @@ __device__ void finish_photon(const KParams &P, const Photon &ph, Counters &cnt)
     }
 }
 
-__device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, Rng &rng, int64_t pid)
+__device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64_t pid)
 {
     // PhotonClass::Init (.cl:344-389) with vStart[0] (.cl:429-467)
     ph.px = P.p0x; ph.py = P.p0y; ph.pz = P.p0z;
     ph.vx = P.v0x; ph.vy = P.v0y; ph.vz = P.v0z;
+    if (P.src_type == 1) {
+        // fibre source (no reference counterpart), event 0: disk of radius src_radius in
+        // the (eX, eY) plane, direction uniform in solid angle within the cone about eZ
+        EventRng rng;
+        rng.draw((uint64_t)pid, 0u, P.stream, P.key0, P.key1);
+        const V3 ex = v3(P.nxx, P.nxy, P.nxz), ey = v3(P.nyx, P.nyy, P.nyz), ez = v3(P.nzx, P.nzy, P.nzz);
+        const float r = P.src_radius * sqrtf(rng.u0);
+        const float phi = 2.0f * 3.14159265358979323846f * rng.u1;
+        const float cp = cosf(phi), sp = sinf(phi);
+        const V3 p = add3(v3(ph.px, ph.py, ph.pz), add3(scl3(r * cp, ex), scl3(r * sp, ey)));
+        ph.px = p.x; ph.py = p.y; ph.pz = p.z;
+        const float ct = 1.0f - rng.u2 * (1.0f - P.src_cos_max);
+        const float stt = sqrtf(1.0f - ct * ct);
+        const float psi = 2.0f * 3.14159265358979323846f * rng.u3;
+        const float cq = cosf(psi), sq = sinf(psi);
+        const V3 v = norm3(add3(scl3(ct, ez), add3(scl3(stt * cq, ex), scl3(stt * sq, ey))));
+        ph.vx = v.x; ph.vy = v.y; ph.vz = v.z;
+    }
     ph.w = P.w0;
     ph.unfin = 0.0f;
     ph.absorbed = 0.0f;
     ph.nvx = 0.0f; ph.nvy = 0.0f; ph.nvz = -1.0f;
-    ph.sft_s = ph.sft_f = ph.sft_t = 0.0f;
+    ph.exit_w = 0.0f;
     ph.curr = 0;
     ph.refTri = -1;
-    ph.fetal = false;
-    ph.roulette = true;
     ph.steps = 0;
+    ph.flags = F_ROULETTE;
     ph.region_acc = 0;
     ph.pid = pid;
-    rng.start((uint64_t)pid);
 }
 
 // One iteration of the reference's do-while loop.  Returns false when the photon ends.
+template <bool Exact>
 __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
-                                            unsigned long long *s_region, Photon &ph, Rng &rng,
-                                            Counters &cnt)
+                                            unsigned long long *s_region, unsigned long long *s_cnt,
+                                            Photon &ph, Counters &cnt)
 {
+    EventRng rng;
+    rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
     const Medium m = s_media[ph.curr];
     float step = 0.0f;
     if (!m.ambient) {
         if (ph.unfin == 0.0f) {
-            float xi;
-            do {
-                xi = rng.next(P.key0, P.key1, P.stream);
-                cnt.draws++;
-            } while (xi <= 0.0f);
-            step = -logf(xi) * P.factor / m.mut;
+            if (Exact) step = -logf(rng.u0) * P.factor / m.mut;
+            else step = -logf(rng.u0) * P.factor * m.inv_mut;
         } else {
-            step = ph.unfin / m.mut;
+            step = Exact ? ph.unfin / m.mut : ph.unfin * m.inv_mut;
             ph.unfin = 0.0f;
         }
     }
@@ -229,11 +292,10 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.py = ph.py + thit * ph.vy;
         ph.pz = ph.pz + thit * ph.vz;
         ph.refTri = -1;
-        const float xi = rng.next(P.key0, P.key1, P.stream);
-        cnt.draws++;
+        const float xi = rng.u1;
         if (tri < 0) {
             // the reference would read mediumIDs[-1] here; the photon leaves the model
-            cnt.miss++;
+            atomicAdd(s_cnt + 4, 1ull);
             ph.w = 0.0f;
         } else {
             const float4 at = __ldg(P.tri_attr + tri);
@@ -250,8 +312,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             }
             ph.nvx = nv.x; ph.nvy = nv.y; ph.nvz = nv.z;
             // TransmitOrReflect (.cl:921-1018)
-            const V3 vin = v3(ph.vx, ph.vy, ph.vz);
-            const float cosIn = dot3(nv, vin);
+            const float cosIn = dot3(nv, v);
             const float absCosIn = fabsf(cosIn);
             const float n1 = m.n, n2 = nx.n;
             float cos_crit = 0.0f;
@@ -259,43 +320,60 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             float r;
             if (absCosIn <= cos_crit) r = 1.0f;
             else r = fresnel(n1, n2, (P.compat & 0x4u) ? cosIn : absCosIn);
-            const V3 e_y = norm3(cross3(nv, cross3(nv, vin)));
             int newID;
             float muaNew, musNew;
             V3 vout;
+            if (Exact) {
+                const V3 e_y = norm3(cross3(nv, cross3(nv, v)));
+                if (xi > r) {
+                    const float sinT = sqrtf(1.0f - cosIn * cosIn) * n1 / n2;
+                    float cosT = -sqrtf(1.0f - sinT * sinT);
+                    if (cosIn > 0.0f) cosT = fabsf(cosT);
+                    vout = norm3(sub3(scl3(cosT, nv), scl3(sinT, e_y)));
+                } else {
+                    const float sinR = sqrtf(1.0f - cosIn * cosIn);
+                    const V3 t = norm3(add3(scl3(cosIn, nv), scl3(sinR, e_y)));
+                    vout = v3(-t.x, -t.y, -t.z);
+                }
+            } else {
+                if (xi > r) {
+                    // v' = cosT n - sinT e_y with e_y = (n cosIn - v) / sinIn (unit n, v)
+                    const float s2 = fmaxf(0.0f, 1.0f - cosIn * cosIn);
+                    const float sinT = sqrtf(s2) * __fdividef(n1, n2);
+                    float cosT = sqrtf(fmaxf(0.0f, 1.0f - sinT * sinT));
+                    if (!(cosIn > 0.0f)) cosT = -cosT;
+                    const float k = s2 > 1e-12f ? sinT * rsqrtf(s2) : 0.0f;
+                    vout = fast_norm(v3(cosT * nv.x - k * (nv.x * cosIn - v.x), cosT * nv.y - k * (nv.y * cosIn - v.y),
+                                        cosT * nv.z - k * (nv.z * cosIn - v.z)));
+                } else {
+                    vout = fast_norm(v3(v.x - 2.0f * cosIn * nv.x, v.y - 2.0f * cosIn * nv.y,
+                                        v.z - 2.0f * cosIn * nv.z));
+                }
+            }
             if (xi > r) {
-                const float sinT = sqrtf(1.0f - cosIn * cosIn) * n1 / n2;
-                float cosT = -sqrtf(1.0f - sinT * sinT);
-                if (cosIn > 0.0f) cosT = fabsf(cosT);
-                vout = norm3(sub3(scl3(cosT, nv), scl3(sinT, e_y)));
                 newID = (cosIn > 0.0f) ? outer : inner;
                 muaNew = nx.mua;
                 musNew = nx.mus;
             } else {
-                const float sinR = sqrtf(1.0f - cosIn * cosIn);
-                const V3 t = norm3(add3(scl3(cosIn, nv), scl3(sinR, e_y)));
-                vout = v3(-t.x, -t.y, -t.z);
                 newID = ph.curr;
                 muaNew = m.mua;
                 musNew = m.mus;
             }
             ph.vx = vout.x; ph.vy = vout.y; ph.vz = vout.z;
             if (muaNew == 0.0f || musNew == 0.0f) {
-                ph.sft_f = 0.0f;
                 const float dist = fabsf(dot3(v3(P.nzx, P.nzy, P.nzz),
                                               v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz)));
-                if (dist > P.distMin) {
-                    ph.sft_t = ph.w * P.exitScale;
-                } else {
-                    if (ph.fetal) ph.sft_f = ph.w * P.exitScale;
-                    ph.sft_s = ph.w * P.exitScale;
-                }
+                uint32_t kind;
+                if (dist > P.distMin) kind = EXIT_TRANS;
+                else kind = (ph.flags & F_FETAL) ? EXIT_SURF_FETAL : EXIT_SURF;
+                ph.exit_w = ph.w * P.exitScale;
+                ph.flags = (ph.flags & ~(3u << EXIT_SHIFT)) | (kind << EXIT_SHIFT);
                 ph.w = 0.0f;
             }
             const int prev = ph.curr;
             ph.curr = newID;
             ph.refTri = tri;
-            if (newID == P.fetal_id) ph.fetal = true;
+            if (newID == P.fetal_id) ph.flags |= F_FETAL;
             ph.unfin = (step - thit) * m.mut;
             if (newID != prev) {
                 if (ph.region_acc) atomicAdd(s_region + prev, ph.region_acc);
@@ -312,10 +390,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             ph.absorbed = ph.w * m.alb;
             ph.w -= ph.absorbed;
         }
-        const float xt = rng.next(P.key0, P.key1, P.stream);
-        const float xp = rng.next(P.key0, P.key1, P.stream);
-        cnt.draws += 2;
-        const V3 vn = vscatter(v3(ph.vx, ph.vy, ph.vz), m.g, xt, xp);
+        const V3 vn = scatter_direction<Exact>(v, m, rng.u1, rng.u2);
         ph.vx = vn.x; ph.vy = vn.y; ph.vz = vn.z;
         const V3 pr = v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz);
         const float cx = dot3(v3(P.nxx, P.nxy, P.nxz), pr);
@@ -324,20 +399,34 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         const float dw = ph.absorbed;
         const unsigned long long fdw = fix32(dw);
         // r-z grid (RecordAbsorbtionRZ, .cl:254-271, with atomic adds and z rows)
-        const float rad = sqrtf(cx * cx + cy * cy) * sign_cl(cx) / P.dg[3];
-        const int row = (int)floorf(cz / P.dg[2]);
-        const int col = (int)floorf(rad + (float)P.dimR);
+        int row, col;
+        if (Exact) {
+            const float rad = sqrtf(cx * cx + cy * cy) * sign_cl(cx) / P.dg[3];
+            row = (int)floorf(cz / P.dg[2]);
+            col = (int)floorf(rad + (float)P.dimR);
+        } else {
+            const float rad = copysignf(sqrtf(cx * cx + cy * cy), cx) * P.inv_dr;
+            row = (int)floorf(cz * P.inv_dz);
+            col = (int)floorf(rad + (float)P.dimR);
+        }
         if (row >= 0 && row < P.rz_nz && col >= 0 && col < P.rz_nr) {
             unsigned long long *c = P.rz + 2 * ((int64_t)row * P.rz_nr + col);
             if (fdw) atomicAdd(c, fdw);
-            if (m.mua > 0.0f) add_fix(c + 1, dw / m.mua);
+            if (m.mua > 0.0f) add_fix(c + 1, Exact ? dw / m.mua : dw * m.inv_mua);
         } else {
             cnt.rz_drop++;
         }
         if (P.vox_nx > 0) {
-            const int ix = (int)floorf(cx / P.vox_dx + 0.5f * (float)P.vox_nx);
-            const int iy = (int)floorf(cy / P.vox_dy + 0.5f * (float)P.vox_ny);
-            const int iz = (int)floorf(cz / P.vox_dz);
+            int ix, iy, iz;
+            if (Exact) {
+                ix = (int)floorf(cx / P.vox_dx + 0.5f * (float)P.vox_nx);
+                iy = (int)floorf(cy / P.vox_dy + 0.5f * (float)P.vox_ny);
+                iz = (int)floorf(cz / P.vox_dz);
+            } else {
+                ix = (int)floorf(cx * P.inv_vdx + 0.5f * (float)P.vox_nx);
+                iy = (int)floorf(cy * P.inv_vdy + 0.5f * (float)P.vox_ny);
+                iz = (int)floorf(cz * P.inv_vdz);
+            }
             if (ix >= 0 && ix < P.vox_nx && iy >= 0 && iy < P.vox_ny && iz >= 0 && iz < P.vox_nz) {
                 if (fdw) atomicAdd(P.vox + ((int64_t)iz * P.vox_ny + iy) * P.vox_nx + ix, fdw);
             } else {
@@ -347,30 +436,28 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.region_acc += fdw;
     }
     if (ph.w < P.w_th && ph.w > 0.0f) {
-        const float xi = rng.next(P.key0, P.key1, P.stream);
-        cnt.draws++;
         cnt.roulette++;
-        if (xi < P.chance) {
+        if (rng.u3 < P.chance) {
             ph.w /= P.chance;
-            ph.roulette = true;
+            ph.flags |= F_ROULETTE;
         } else {
             ph.w = 0.0f;
-            ph.roulette = false;
+            ph.flags &= ~F_ROULETTE;
         }
     }
     ph.steps++;
     if (P.max_steps > 0 && (int64_t)ph.steps >= P.max_steps && ph.w > 0.0f) {
-        cnt.capped++;
+        atomicAdd(s_cnt + 5, 1ull);
         ph.w = 0.0f;
     }
-    return ph.w > 0.0f && (ph.w > P.w_th || ph.roulette);
+    return ph.w > 0.0f && (ph.w > P.w_th || (ph.flags & F_ROULETTE));
 }
 
 struct SmemLayout {
     int off_media, off_region, off_cnt, off_na, off_nb, off_nc, off_nd, off_ta, off_tb, off_tc, bytes;
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int n_media, int nodes_smem, int tris_smem)
+__host__ __device__ inline SmemLayout smem_layout(int nodes_smem, int tris_smem)
 {
     SmemLayout L;
     int o = 0;
@@ -385,11 +472,10 @@ __host__ __device__ inline SmemLayout smem_layout(int n_media, int nodes_smem, i
     L.off_tb = o; o += tris_smem * 16;
     L.off_tc = o; o += tris_smem * 16;
     L.bytes = o;
-    (void)n_media;
     return L;
 }
 
-__device__ MeshView stage_mesh(const KParams &P, unsigned char *smem, const SmemLayout &L)
+__device__ __forceinline__ MeshView stage_mesh(const KParams &P, unsigned char *smem, const SmemLayout &L)
 {
     MeshView M;
     M.na = P.node_a; M.nb = P.node_b; M.nc = P.node_c; M.nd = P.node_d;
@@ -414,10 +500,11 @@ __device__ MeshView stage_mesh(const KParams &P, unsigned char *smem, const Smem
     return M;
 }
 
-__global__ void __launch_bounds__(kBlock) transport_kernel(const __grid_constant__ KParams P)
+template <bool Exact>
+__global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_constant__ KParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const SmemLayout L = smem_layout(P.n_media, P.nodes_smem, P.tris_smem);
+    const SmemLayout L = smem_layout(P.nodes_smem, P.tris_smem);
     Medium *s_media = reinterpret_cast<Medium *>(smem + L.off_media);
     unsigned long long *s_region = reinterpret_cast<unsigned long long *>(smem + L.off_region);
     unsigned long long *s_cnt = reinterpret_cast<unsigned long long *>(smem + L.off_cnt);
@@ -432,8 +519,8 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(const __grid_constant
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
     Counters cnt = {};
+    uint32_t photons = 0;
     Photon ph;
-    Rng rng;
     bool alive = false;
     bool exhausted = false;
     for (;;) {
@@ -447,28 +534,34 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(const __grid_constant
             if (!alive) {
                 const unsigned long long idx = base + __popc(need & lt_mask);
                 if (idx < (unsigned long long)P.n) {
-                    start_photon(P, ph, rng, P.first + (int64_t)idx);
+                    start_photon(P, ph, P.first + (int64_t)idx);
                     alive = true;
                 }
             }
         }
         if (!__any_sync(0xffffffffu, alive)) break;
         if (alive) {
-            if (!step_photon(P, M, s_media, s_region, ph, rng, cnt)) {
+            if (!step_photon<Exact>(P, M, s_media, s_region, s_cnt, ph, cnt)) {
                 if (ph.region_acc) atomicAdd(s_region + ph.curr, ph.region_acc);
-                finish_photon(P, ph, cnt);
+                finish_photon(P, ph);
+                photons++;
                 alive = false;
             }
         }
     }
     // block-level reduction of counters and region sums
-    const uint32_t cv[10] = {cnt.scatter, cnt.boundary, cnt.query, cnt.roulette, cnt.miss,
-                             cnt.capped, cnt.rz_drop, cnt.vox_drop, cnt.photons, cnt.draws};
+    const uint32_t cv[8] = {cnt.scatter, cnt.boundary, cnt.query, cnt.roulette, 0u, 0u, cnt.rz_drop, cnt.vox_drop};
 #pragma unroll
-    for (int i = 0; i < 10; ++i) {
+    for (int i = 0; i < 8; ++i) {
+        if (i == 4 || i == 5) continue;
         unsigned long long x = cv[i];
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0 && x) atomicAdd(s_cnt + i, x);
+    }
+    {
+        unsigned long long x = photons;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0 && x) atomicAdd(s_cnt + 8, x);
     }
     __syncthreads();
     if (threadIdx.x < 16 && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);
@@ -476,123 +569,19 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(const __grid_constant
         if (s_region[i]) atomicAdd(P.region + i, s_region[i]);
 }
 
-__global__ void __launch_bounds__(kBlock) query_kernel(const __grid_constant__ KParams P, int64_t n,
-                                                       const float *orig, const float *dir,
-                                                       const int32_t *ref, const float *tmax,
-                                                       int32_t *id_out, float *t_out)
+template <bool Exact>
+cudaError_t launch_transport_t(const KParams &P, int grid, int smem, cudaStream_t s)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const SmemLayout L = smem_layout(P.n_media, P.nodes_smem, P.tris_smem);
-    const MeshView M = stage_mesh(P, smem, L);
-    __syncthreads();
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const V3 p = v3(orig[3 * i], orig[3 * i + 1], orig[3 * i + 2]);
-        const V3 v = v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
-        float t;
-        id_out[i] = query_nearest(M, p, v, ref[i], tmax[i], t);
-        t_out[i] = t;
-    }
-}
-
-__global__ void philox_kernel(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
-                              uint32_t k1, int64_t n, uint32_t *out)
-{
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t a = c0, b = c1, c = c2 + (uint32_t)i, d = c3;
-        philox4x32_10(a, b, c, d, k0, k1);
-        out[4 * i] = a; out[4 * i + 1] = b; out[4 * i + 2] = c; out[4 * i + 3] = d;
-    }
-}
-
-// ------------------------------------------------------------- host launchers
-int smem_bytes(int n_media, int nodes_smem, int tris_smem)
-{
-    return smem_layout(n_media, nodes_smem, tris_smem).bytes;
-}
-
-cudaError_t launch_transport(const KParams &P, int grid, int smem, cudaStream_t s)
-{
-    transport_kernel<<<grid, kBlock, smem, s>>>(P);
+    transport_kernel<Exact><<<grid, kBlock, smem, s>>>(P);
     return cudaGetLastError();
 }
 
-cudaError_t transport_occupancy(int smem, int *blocks_per_sm)
+template <bool Exact>
+cudaError_t transport_occupancy_t(int smem, int *blocks_per_sm)
 {
-    cudaError_t e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(transport_kernel<Exact>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, kBlock, smem);
-}
-
-cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *orig, const float *dir,
-                         const int32_t *ref, const float *tmax, int32_t *id_out, float *t_out,
-                         cudaStream_t s)
-{
-    cudaError_t e = cudaFuncSetAttribute(query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    int grid = (int)std::min<int64_t>((n + kBlock - 1) / kBlock, 148 * 8);
-    if (grid < 1) grid = 1;
-    query_kernel<<<grid, kBlock, smem, s>>>(P, n, orig, dir, ref, tmax, id_out, t_out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out,
-                          cudaStream_t s)
-{
-    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    if (grid < 1) grid = 1;
-    philox_kernel<<<grid, 256, 0, s>>>(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1], n, out);
-    return cudaGetLastError();
-}
-
-int block_size() { return kBlock; }
-
-}  // namespace lp
-
-namespace lp {
-
-// FP32 throughput probe: 8 independent FMA chains per thread (__fmaf_rn, so the
-// file-wide --fmad=false does not split them).  2 flops per FMA.
-__global__ void __launch_bounds__(256) fma_peak_kernel(float *out, int iters, float a, float b)
-{
-    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
-    float x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
-    for (int i = 0; i < iters; ++i) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            x0 = __fmaf_rn(x0, a, b); x1 = __fmaf_rn(x1, a, b); x2 = __fmaf_rn(x2, a, b); x3 = __fmaf_rn(x3, a, b);
-            x4 = __fmaf_rn(x4, a, b); x5 = __fmaf_rn(x5, a, b); x6 = __fmaf_rn(x6, a, b); x7 = __fmaf_rn(x7, a, b);
-        }
-    }
-    const float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
-    if (s == 1234.5f) out[0] = s;  // keeps the chains alive; practically never taken
-}
-
-double fma_peak_tflops(int num_sms)
-{
-    float *d = nullptr;
-    if (cudaMalloc(&d, 16) != cudaSuccess) return 0.0;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    const int blocks = num_sms * 8, threads = 256, iters = 4096;
-    fma_peak_kernel<<<blocks, threads>>>(d, 64, 0.999f, 1e-3f);  // warm-up
-    double best = 0.0;
-    for (int r = 0; r < 3; ++r) {
-        cudaEventRecord(e0);
-        fma_peak_kernel<<<blocks, threads>>>(d, iters, 0.999f, 1e-3f);
-        cudaEventRecord(e1);
-        cudaEventSynchronize(e1);
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
-        if (ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(d);
-    return best;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<Exact>, kBlock, smem);
 }
 
 }  // namespace lp

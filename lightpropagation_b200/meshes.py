@@ -55,6 +55,182 @@ def face_normals(tri: np.ndarray) -> np.ndarray:
     return n.astype(F)
 
 
+def geodesic_sphere(freq: int):
+    """Unit sphere from an icosahedron whose faces are split into freq^2 triangles.
+
+    Returns vertices [V,3] (float64, unit length) and faces [20*freq^2, 3] (int, counter-
+    clockwise seen from outside).  Vertices on shared icosahedron edges are created once,
+    so neighbouring triangles share bit-identical edge vertices."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    ico_v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                      [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    ico_v /= np.linalg.norm(ico_v, axis=1, keepdims=True)
+    ico_f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    n = int(freq)
+    verts = [v for v in ico_v]
+    key_to_id = {("c", i): i for i in range(12)}
+
+    def vid(face, i, j):
+        a, b, c = face
+        k = n - i - j
+        # canonical key: a corner, a point on an edge (by sorted endpoints), or a face-interior point
+        if i == n:
+            return key_to_id[("c", b)]
+        if j == n:
+            return key_to_id[("c", c)]
+        if k == n:
+            return key_to_id[("c", a)]
+        if k == 0:
+            e, s = (b, c), j
+        elif i == 0:
+            e, s = (a, c), j
+        elif j == 0:
+            e, s = (a, b), i
+        else:
+            e = None
+        if e is not None:
+            lo, hi = min(e), max(e)
+            pos = s if e[0] == lo else n - s
+            key = ("e", lo, hi, pos)
+            if key not in key_to_id:
+                p = ico_v[lo] * (n - pos) / n + ico_v[hi] * pos / n
+                key_to_id[key] = len(verts)
+                verts.append(p / np.linalg.norm(p))
+            return key_to_id[key]
+        key = ("f", face, i, j)
+        if key not in key_to_id:
+            p = ico_v[a] * k / n + ico_v[b] * i / n + ico_v[c] * j / n
+            key_to_id[key] = len(verts)
+            verts.append(p / np.linalg.norm(p))
+        return key_to_id[key]
+
+    faces = []
+    for f in ico_f:
+        for i in range(n):
+            for j in range(n - i):
+                faces.append((vid(f, i, j), vid(f, i + 1, j), vid(f, i, j + 1)))
+                if i + j < n - 1:
+                    faces.append((vid(f, i + 1, j), vid(f, i + 1, j + 1), vid(f, i, j + 1)))
+    return np.array(verts, np.float64), np.array(faces, np.int64)
+
+
+def smooth_noise(u: np.ndarray, seed: int, terms: int = 12, freq: float = 2.0) -> np.ndarray:
+    """Seeded smooth scalar field on the unit sphere, scaled to [0, 1]."""
+    rng = np.random.default_rng(seed)
+    k = rng.normal(size=(terms, 3))
+    k *= freq / np.linalg.norm(k, axis=1, keepdims=True)
+    ph = rng.uniform(0, 2 * np.pi, terms)
+    amp = rng.uniform(0.5, 1.0, terms)
+    s = (amp[None, :] * np.cos(u @ k.T + ph[None, :])).sum(1)
+    return (s - s.min()) / (s.max() - s.min())
+
+
+def _shell_triangles(points: np.ndarray, faces: np.ndarray, inner: int, outer: int):
+    tri = points[faces].reshape(-1, 9).astype(F)
+    med = np.tile(np.array([[inner, outer]], np.int32), (faces.shape[0], 1))
+    return tri, med
+
+
+def curved_abdomen(freq: int = 45, axes=(150.0, 120.0, 100.0), skin=2.0, fat=(8.0, 15.0), uterus=10.0,
+                   head_radius=45.0, head_depth=40.0, noise_seed=2):
+    """Nested shells of a maternal ellipsoid plus a fetal head sphere.
+
+    Regions: 0 ambient, 1 skin, 2 fat, 3 uterus, 4 amniotic fluid, 5 fetal head.
+    The outer ellipsoid (semi-axes a, b, c) is offset inwards along its normal by the
+    skin thickness, then by a fat thickness that varies smoothly in [fat[0], fat[1]]
+    (seeded noise over the sphere), then by the uterus thickness; inside lies the
+    amniotic fluid.  The head sphere sits on the -z axis below the source at z = -c,
+    its nearest surface head_depth below the skin.  Every surface is a geodesic
+    sphere of the given frequency (20 * freq^2 triangles), so freq = 45 gives
+    5 x 40500 = 202,500 triangles.  Normals point outwards (inner -> outer region)."""
+    a, b, c = axes
+    u, faces = geodesic_sphere(freq)
+    p0 = u * np.array([a, b, c])[None, :]
+    nrm = p0 / np.array([a * a, b * b, c * c])[None, :]
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    t_fat = fat[0] + (fat[1] - fat[0]) * smooth_noise(u, noise_seed)
+    depths = [np.zeros(len(u)), np.full(len(u), skin), skin + t_fat, skin + t_fat + uterus]
+    regions = [(1, 0), (2, 1), (3, 2), (4, 3)]
+    tris, meds = [], []
+    for d, (inner, outer) in zip(depths, regions):
+        pts = p0 - d[:, None] * nrm
+        t, m = _shell_triangles(pts, faces, inner, outer)
+        tris.append(t)
+        meds.append(m)
+    centre = np.array([0.0, 0.0, -c + head_depth + head_radius])
+    t, m = _shell_triangles(centre[None, :] + head_radius * u, faces, 5, 4)
+    tris.append(t)
+    meds.append(m)
+    tri = np.concatenate(tris)
+    med = np.concatenate(meds)
+    return tri, face_normals(tri), med
+
+
+def write_obj(path, tri: np.ndarray, med: np.ndarray, names) -> None:
+    """Write a mesh in the reference's OBJ convention (ImportExport.cpp:952-1053):
+    runs of triangles with the same (inner, outer) pair become `o <names[inner]>`,
+    `g <outer>` and one `f` line per triangle (vertex order kept, so normals keep
+    their orientation).  Vertices are written with 9 significant digits, which
+    round-trips float32 exactly."""
+    tri = np.asarray(tri, F).reshape(-1, 9)
+    med = np.asarray(med, np.int32).reshape(-1, 2)
+    with open(path, "w") as f:
+        f.write("# written by lightpropagation_b200.meshes.write_obj\n")
+        for v in tri.reshape(-1, 3):
+            f.write("v %.9g %.9g %.9g\n" % (v[0], v[1], v[2]))
+        last = None
+        for i, (inner, outer) in enumerate(med):
+            if last is None or inner != last[0]:
+                f.write(f"o {names[inner]}\n")
+                last = None
+            if last is None or outer != last[1]:
+                f.write(f"g {outer}\n")
+            f.write(f"f {3 * i + 1} {3 * i + 2} {3 * i + 3}\n")
+            last = (inner, outer)
+
+
+def write_config(path, model_file, tissues, dims, det_grid, emitter_pos, emitter_heading, distance,
+                 photons, fetal_id, chance=0.1, w_threshold=1e-4, ppu=1.0, emitter_file="emitter.txt"):
+    """Write a <config> XML with the keys ReadXML reads (src/IO/ReadXML.cpp:109-870).
+    tissues: list of (name, n, mua, mus, g) in region order."""
+    t = "\n".join(
+        f"      <tissue><ID>{i}</ID><name>{nm}</name><anisotropy>{g}</anisotropy><mua>{mua}</mua>"
+        f"<mus>{mus}</mus><refraction>{n}</refraction></tissue>" for i, (nm, n, mua, mus, g) in enumerate(tissues))
+    xyz = lambda v: "".join(f"<{k}>{x}</{k}>" for k, x in zip("xyz", v))
+    g = "".join(f"<{k}>{x}</{k}>" for k, x in zip(("x", "y", "z", "r", "phi", "rho"), det_grid))
+    with open(path, "w") as f:
+        f.write(f"""<?xml version='1.0' encoding="utf-8"?>
+<config>
+  <model>
+    <modelfile>{model_file}</modelfile>
+    <unit>mm</unit>
+    <PixelPerUnit>{ppu}</PixelPerUnit>
+    <dimensions>{xyz(dims)}</dimensions>
+    <tissueList>
+{t}
+    </tissueList>
+  </model>
+  <Emittermodel>
+    <file>{emitter_file}</file>
+    <position>{xyz(emitter_pos)}</position>
+    <distance>{distance}</distance>
+    <heading>{xyz(emitter_heading)}</heading>
+  </Emittermodel>
+  <SimulationParams>
+    <numberOfPhotons>{photons}</numberOfPhotons>
+    <chance>{chance}</chance>
+    <weightThreshold>{w_threshold}</weightThreshold>
+  </SimulationParams>
+  <Logs>
+    <fetalID>{fetal_id}</fetalID>
+    <DetectionGrid>{g}</DetectionGrid>
+  </Logs>
+</config>
+""")
+
+
 def _quad(p0, p1, p2, p3):
     """Two triangles of the planar quad p0-p1-p2-p3 (counter-clockwise seen from the normal side)."""
     return [p0 + p1 + p2, p0 + p2 + p3]

@@ -88,6 +88,9 @@ class Simulation:
         occ = _i32(v_occ if v_occ is not None else [1] * (v.size // 3))
         self._ck(self._L.lp_set_source(self._h, N.fptr(p), N.fptr(v), N.iptr(occ), v.size // 3, N.fptr(e)))
 
+    def set_fiber_source(self, radius: float, na: float):
+        self._ck(self._L.lp_set_fiber_source(self._h, float(radius), float(na)))
+
     def set_tally_grid(self, dimensions, det_grid, fetal_id: int):
         d, g = _f32(dimensions, 3), _f32(det_grid, 6)
         self._ck(self._L.lp_set_tally_grid(self._h, N.fptr(d), N.fptr(g), int(fetal_id)))
@@ -100,6 +103,10 @@ class Simulation:
         dr = _f32(det_r if det_r is not None else np.zeros((0, 2)))
         self._ck(self._L.lp_set_extra_tallies(self._h, N.iptr(vn), N.fptr(vd), int(n_rbins), float(rbin_dr),
                                               dr.size // 2, N.fptr(dr)))
+
+    def set_arithmetic(self, exact: bool):
+        """exact=True: the reference kernel's operation order; False (default): fast."""
+        self._ck(self._L.lp_set_arithmetic(self._h, 1 if exact else 0))
 
     def set_max_steps(self, n: int):
         self._ck(self._L.lp_set_max_steps(self._h, int(n)))

@@ -42,19 +42,34 @@ class Workload:
     rbin_dr: float = 1.0
     det_r: Optional[np.ndarray] = None
     region_names: list = field(default_factory=list)
+    fiber_radius: float = 0.0
+    fiber_na: float = 0.0
+    # reference behaviours kept (LP_COMPAT_*): 7 keeps all of them (the reference's own
+    # pencil-beam layouts); 0 uses the corrected physics, needed wherever light enters a
+    # region obliquely against a face normal (the signed-cosine Fresnel of the
+    # reference reflects every such photon)
+    compat: int = 7
 
     @property
     def n_tri(self) -> int:
         return int(self.tri.shape[0])
 
-    def apply(self, sim, seed=0x4C50, compat=7):
+    @property
+    def src_cos_max(self) -> float:
+        """cos of the fibre cone half-angle, in float32 as the library computes it."""
+        s = np.float32(self.fiber_na) / np.float32(self.nmuasg[0, 0])
+        return float(np.sqrt(np.float32(1.0) - s * s))
+
+    def apply(self, sim, seed=0x4C50, compat=None):
         """Load this workload into a propagation.Simulation."""
+        compat = self.compat if compat is None else compat
         sim.set_mesh(self.tri, self.nrm, self.med)
         sim.set_media(self.nmuasg)
         sim.set_source(self.p_start, self.v_start, self.ep0xyz)
         sim.set_tally_grid(self.dimensions, self.det_grid, self.fetal_id)
         sim.set_params(self.chance, self.w_threshold, self.factor, seed, compat)
         sim.set_extra_tallies(self.vox_n, self.vox_d, self.n_rbins, self.rbin_dr, self.det_r)
+        sim.set_fiber_source(self.fiber_radius, self.fiber_na)
         return sim
 
 
@@ -83,4 +98,47 @@ def plain_slab(n_photons: int = 1_000_000) -> Workload:
         region_names=["ambient", "skin", "fat", "uterus"])
 
 
-WORKLOADS = {"plain_slab": plain_slab}
+# Optical properties of the abdomen regions (n, mua [1/mm], mus [1/mm], g) at the two
+# wavelengths.  Synthetic values in the usual literature ranges for skin, fat, uterine
+# wall and fetal head; the amniotic fluid values are the benchmark's own.  They are
+# inputs of the benchmark, not measurements.
+ABDOMEN_MEDIA = {
+    660: [[1.0, 0.0, 0.0, 0.0],        # ambient
+          [1.4, 0.02, 20.0, 0.9],      # skin
+          [1.44, 0.003, 12.0, 0.9],    # fat
+          [1.4, 0.02, 8.0, 0.9],       # uterus
+          [1.33, 0.001, 0.1, 0.9],     # amniotic fluid
+          [1.4, 0.015, 10.0, 0.9]],    # fetal head
+    940: [[1.0, 0.0, 0.0, 0.0],
+          [1.4, 0.015, 15.0, 0.9],
+          [1.44, 0.004, 10.0, 0.9],
+          [1.4, 0.025, 7.0, 0.9],
+          [1.33, 0.001, 0.1, 0.9],
+          [1.4, 0.02, 8.0, 0.9]],
+}
+RING_SEPARATIONS_MM = (20.0, 36.0, 52.0, 68.0, 84.0, 100.0)
+
+
+def curved_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int = 45) -> Workload:
+    """Curved mesh abdomen: maternal ellipsoid (semi-axes 150/120/100 mm) with nested
+    skin (2 mm), fat (8-15 mm, seeded smooth noise), uterus (10 mm) shells, amniotic
+    fluid inside, and a fetal head sphere (radius 45 mm, nearest surface 40 mm below the
+    skin); 5 x 20 * freq^2 triangles (202,500 at freq 45).  A 0.4 mm NA-0.22 fibre at the
+    -z pole points into the body; six 1 mm wide ring detectors at 20-100 mm."""
+    tri, nrm, med = meshes.curved_abdomen(freq=freq)
+    nmuasg = np.array(ABDOMEN_MEDIA[int(wavelength)], F)
+    p0, v0, ep = pencil_source(poi=(0.0, 0.0, -100.0), heading=(0.0, 0.0, 1.0), distance=1.0)
+    det_r = np.array([[r - 0.5, r + 0.5] for r in RING_SEPARATIONS_MM], F)
+    return Workload(
+        name=f"curved_abdomen_{wavelength}nm_{tri.shape[0]}tri", tri=tri, nrm=nrm, med=med, nmuasg=nmuasg,
+        p_start=p0, v_start=v0, ep0xyz=ep,
+        dimensions=np.array([300.0, 240.0, 200.0], F),
+        det_grid=np.array([1.0, 1.0, 1.0, 0.5, 1.0, 1.0], F),
+        fetal_id=5, n_photons=n_photons,
+        vox_n=(200, 200, 120), vox_d=(1.0, 1.0, 1.0), n_rbins=300, rbin_dr=0.5, det_r=det_r,
+        region_names=["ambient", "skin", "fat", "uterus", "amniotic", "fetal_head"],
+        fiber_radius=0.2, fiber_na=0.22, compat=0)
+
+
+WORKLOADS = {"plain_slab": plain_slab, "curved_abdomen": curved_abdomen,
+             "curved_abdomen_940": lambda n_photons=10_000_000: curved_abdomen(n_photons, 940)}

@@ -141,9 +141,11 @@ typedef struct {
     int32_t own_ix[3];
     /* philox */
     uint32_t key[2], ctr[4], buf[4];
-    int used;
     uint64_t draws;
 } rng_t;
+
+/* Draw slots of one transport event (shared with the CUDA path). */
+enum { SLOT_STEP = 0, SLOT_ANGLE = 1, SLOT_AZIMUTH = 2, SLOT_ROULETTE = 3 };
 
 static void rng_photon(rng_t *r, const lpo_problem *P, int64_t pid)
 {
@@ -154,29 +156,34 @@ static void rng_photon(rng_t *r, const lpo_problem *P, int64_t pid)
         r->st = r->own_st;
         r->ix = r->own_ix;
     } else if (r->mode == LPO_RNG_PHILOX) {
-        /* Counter layout shared with the CUDA path: (photon lo, photon hi, block, stream). */
         r->key[0] = (uint32_t)P->seed;
         r->key[1] = (uint32_t)(P->seed >> 32);
         r->ctr[0] = (uint32_t)(uint64_t)pid;
         r->ctr[1] = (uint32_t)((uint64_t)pid >> 32);
         r->ctr[2] = 0;
         r->ctr[3] = P->stream;
-        r->used = 4;
     }
 }
 
-static inline float rng_next(rng_t *r)
+/* Philox layout shared with the CUDA path: one Philox4x32-10 block per event,
+ * counter = (photon lo, photon hi, event, stream), key = seed.  Event 0 samples the
+ * source; transport loop iteration i (0-based) is event i + 1.  The block's four
+ * words are the event's draw slots (step, Fresnel or polar angle, azimuth,
+ * roulette), each mapped to the odd multiple of 2^-24 ((x >> 8) | 1) * 2^-24, a
+ * uniform in (0, 1).  The ran3 modes ignore events and slots and draw in order,
+ * which is the reference's draw order within an event. */
+static inline void rng_event(rng_t *r, uint32_t ev)
+{
+    if (r->mode == LPO_RNG_PHILOX) {
+        r->ctr[2] = ev;
+        lpo_philox4x32_10(r->ctr, r->key, r->buf);
+    }
+}
+
+static inline float rng_slot(rng_t *r, int slot)
 {
     r->draws++;
-    if (r->mode == LPO_RNG_PHILOX) {
-        if (r->used == 4) {
-            lpo_philox4x32_10(r->ctr, r->key, r->buf);
-            r->ctr[2]++;
-            r->used = 0;
-        }
-        uint32_t x = r->buf[r->used++];
-        return (float)(x >> 8) * 0x1.0p-24f;
-    }
+    if (r->mode == LPO_RNG_PHILOX) return (float)((r->buf[slot] >> 8) | 1u) * 0x1.0p-24f;
     return lpo_ran3_draw(r->st, r->ix);
 }
 
@@ -501,6 +508,20 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
     /* PhotonClass::Init (.cl:344-389) with vStart[0] (.cl:429-467) */
     ph.v = mk(P->v_start[0], P->v_start[1], P->v_start[2]);
     ph.p = mk(P->p_start[0], P->p_start[1], P->p_start[2]);
+    if (P->src_type == 1) {
+        /* fibre source (extension, see lp_oracle.h), event 0 */
+        rng_event(R, 0);
+        float x1 = rng_slot(R, 0), x2 = rng_slot(R, 1), x3 = rng_slot(R, 2), x4 = rng_slot(R, 3);
+        float r = P->src_radius * sqrtf(x1);
+        float phi = 2 * PI_F * x2;
+        float cp = cosf(phi), sp = sinf(phi);
+        ph.p = add(ph.p, add(scl(r * cp, C->nX), scl(r * sp, C->nY)));
+        float ct = 1.0f - x3 * (1.0f - P->src_cos_max);
+        float stt = sqrtf(1.0f - ct * ct);
+        float psi = 2 * PI_F * x4;
+        float cq = cosf(psi), sq = sinf(psi);
+        ph.v = normalize(add(scl(ct, C->nZ), add(scl(stt * cq, C->nX), scl(stt * sq, C->nY))));
+    }
     ph.w = 1.0f - C->Rsp;
     ph.SFT = mk(0, 0, 0);
     ph.stepsize = 0.0f;
@@ -518,12 +539,13 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
         float pp[3] = {ph.p.x, ph.p.y, ph.p.z}, vv[3] = {ph.v.x, ph.v.y, ph.v.z};
         int triID = lpo_find_triangle(P->tri, P->n_tri, ph.refTri, pp, vv, &ph.steptoboundary);
         T->counters[LPO_C_QUERY]++;
+        rng_event(R, (uint32_t)(steps + 1));
         const float *cur = nm + 4 * curr;
         if (cur[1] == 0.0f && cur[2] == 0.0f) {
             ph.stepsize = ph.steptoboundary;
         } else if (ph.unfin == 0.0f) {
             float xi;
-            do { xi = rng_next(R); } while (xi <= 0.0f);
+            do { xi = rng_slot(R, SLOT_STEP); } while (xi <= 0.0f);
             ph.stepsize = -logf(xi) * P->factor / (cur[1] + cur[2]);
         } else {
             ph.stepsize = ph.unfin / (cur[1] + cur[2]);
@@ -533,7 +555,7 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
             T->counters[LPO_C_BOUNDARY]++;
             ph.p = add(ph.p, scl(ph.steptoboundary, ph.v));
             ph.refTri = -1;
-            float xi = rng_next(R);
+            float xi = rng_slot(R, SLOT_ANGLE);
             if (triID < 0) {
                 /* no triangle ahead: the reference reads mediumIDs[-1]; here the photon leaves */
                 T->counters[LPO_C_MISS]++;
@@ -566,8 +588,8 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
                 ph.absorbed = ph.w * (cur[1] / (cur[1] + cur[2]));
                 ph.w -= ph.absorbed;
             }
-            float xt = rng_next(R);
-            float xp = rng_next(R);
+            float xt = rng_slot(R, SLOT_ANGLE);
+            float xp = rng_slot(R, SLOT_AZIMUTH);
             vscatter(&ph, cur[3], xt, xp);
             f3 pr = sub(ph.p, C->POI);
             f3 coords = mk(dot(C->nX, pr), dot(C->nY, pr), dot(C->nZ, pr));
@@ -575,7 +597,7 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
             region_acc += lpo_fix(ph.absorbed);
         }
         if (ph.w < P->w_threshold && ph.w > 0.0f) {
-            float xi = rng_next(R);
+            float xi = rng_slot(R, SLOT_ROULETTE);
             T->counters[LPO_C_ROULETTE]++;
             if (xi < P->chance) {
                 ph.w /= P->chance;

@@ -92,6 +92,13 @@ typedef struct lpo_problem {
     float rbin_dr;
     int32_t n_det;
     const float *det_r;     /* n_det x (r_lo, r_hi) annuli of the exit radius    */
+    /* source extension (no reference counterpart): 0 = pencil beam as in the
+     * reference, 1 = fibre: start point uniform on a disk of radius src_radius
+     * around p_start in the (eX, eY) plane, direction uniform in solid angle
+     * within the cone cos(theta) >= src_cos_max around eZ.  Four draws
+     * (r, phi, cos theta, psi) open the photon's stream. */
+    int32_t src_type;
+    float src_radius, src_cos_max;
 } lpo_problem;
 
 typedef struct lpo_geometry {

@@ -46,6 +46,7 @@ class Problem(C.Structure):
         ("vox_n", C.c_int32 * 3), ("vox_d", C.c_float * 3),
         ("n_rbins", C.c_int32), ("rbin_dr", C.c_float),
         ("n_det", C.c_int32), ("det_r", _fp),
+        ("src_type", C.c_int32), ("src_radius", C.c_float), ("src_cos_max", C.c_float),
     ]
 
 
@@ -155,6 +156,9 @@ class Case:
     n_rbins: int = 0
     rbin_dr: float = 1.0
     det_r: Optional[np.ndarray] = None   # float32 [D, 2]
+    src_type: int = 0
+    src_radius: float = 0.0
+    src_cos_max: float = 1.0
     keep: list = field(default_factory=list, repr=False)
 
     def problem(self, rng_mode=RNG_PHILOX, seed=0x4C50, compat=COMPAT_ALL, stream=0,
@@ -181,6 +185,7 @@ class Case:
         P.n_rbins, P.rbin_dr = self.n_rbins, self.rbin_dr
         P.n_det = det_r.shape[0]
         P.det_r = fptr(det_r)
+        P.src_type, P.src_radius, P.src_cos_max = self.src_type, self.src_radius, self.src_cos_max
         return P
 
 

@@ -21,7 +21,9 @@ def to_case(w) -> "po.Case":
                    v_start=w.v_start, ep0xyz=w.ep0xyz, dimensions=w.dimensions,
                    det_grid=w.det_grid, fetal_id=w.fetal_id, chance=w.chance,
                    w_threshold=w.w_threshold, factor=w.factor, vox_n=w.vox_n, vox_d=w.vox_d,
-                   n_rbins=w.n_rbins, rbin_dr=w.rbin_dr, det_r=w.det_r)
+                   n_rbins=w.n_rbins, rbin_dr=w.rbin_dr, det_r=w.det_r,
+                   src_type=1 if (w.fiber_radius > 0 or w.fiber_na > 0) else 0,
+                   src_radius=w.fiber_radius, src_cos_max=w.src_cos_max)
 
 
 @pytest.fixture(scope="session")

@@ -1,13 +1,15 @@
 """CUDA path against the CPU oracle (marked gpu: run on a B200).
 
-Three levels of agreement are checked:
+Levels of agreement checked:
   * exact:  Philox blocks, BVH nearest-triangle queries (id and distance bits), and
             run-to-run / split-run determinism of the fixed-point tallies;
-  * common random numbers: with the same seed the GPU and the oracle consume the
-            same random numbers per photon, so per-photon exit records agree except
-            where a last-place difference of logf/cosf/acosf flips a decision;
-  * statistical: independent seeds, batch means, |z| < 3 per scalar tally
-            (4.5 for image bins, with at most 1% of bins above 3).
+  * common random numbers: in the reference-arithmetic mode (lp_set_arithmetic(1)) the
+            GPU and the oracle consume the same random numbers per photon and follow the
+            same trajectory except where a last-place difference of logf/cosf/acosf
+            flips a decision;
+  * statistical: the production (fast) mode against the oracle with independent
+            streams, batch means, |z| < 3 per scalar tally and |z| < 4.5 per image bin;
+            and fast against reference arithmetic on the GPU at high statistics.
 """
 import numpy as np
 import pytest
@@ -26,9 +28,17 @@ def slab():
     return workloads.plain_slab()
 
 
-def gpu_run(w, n, seed, first=0, exit_records=0, compat=7):
+@pytest.fixture(scope="module")
+def abdomen_small():
+    # the curved abdomen at a coarse tessellation (5 x 720 triangles) so the brute-force
+    # oracle stays fast; same regions, optics, fibre source and ring detectors
+    return workloads.curved_abdomen(wavelength=660, freq=6)
+
+
+def gpu_run(w, n, seed, first=0, exit_records=0, exact=False, compat=None):
     with Simulation(0) as s:
         w.apply(s, seed=seed, compat=compat)
+        s.set_arithmetic(exact)
         if exit_records:
             s.set_exit_records(exit_records)
         s.zero()
@@ -36,6 +46,13 @@ def gpu_run(w, n, seed, first=0, exit_records=0, compat=7):
         t = s.tallies()
         rec = s.exit_records(exit_records) if exit_records else None
     return t, rec
+
+
+def scalars(sft, region, det=None):
+    v = [sft[:, :, 0].sum(), sft[:, :, 1].sum(), sft[:, :, 2].sum()] + list(region[1:])
+    if det is not None and len(det):
+        v += list(det[:, 0])
+    return np.array(v, np.float64)
 
 
 def test_philox_matches_oracle(oracle_lib):
@@ -49,35 +66,38 @@ def test_philox_matches_oracle(oracle_lib):
 
 
 def _soup(rng, n):
-    """Random triangle soup with some shared edges and coincident pairs."""
+    """Random triangle soup with exact duplicates and shared vertices."""
     c = rng.uniform(-20, 20, (n, 1, 3))
     t = (c + rng.normal(scale=3.0, size=(n, 3, 3))).astype(np.float32)
-    t[1::7] = t[0::7][: t[1::7].shape[0]]                        # exact duplicates
-    t[2::5, 0] = t[3::5, 1][: t[2::5].shape[0]]                   # shared vertices
+    t[1::7] = t[0::7][: t[1::7].shape[0]]
+    t[2::5, 0] = t[3::5, 1][: t[2::5].shape[0]]
     return t.reshape(n, 9)
 
 
-@pytest.mark.parametrize("mesh", ["slab", "soup"])
+@pytest.mark.parametrize("mesh", ["slab", "soup", "abdomen"])
 def test_bvh_query_matches_brute_force(oracle_lib, mesh):
     rng = np.random.default_rng(11)
     if mesh == "slab":
         tri, nrm, med = meshes.layered_slab([2.0, 10.0, 30.0])
         lo, hi = np.array([-55, -55, -5]), np.array([55, 55, 47])
-    else:
+    elif mesh == "soup":
         tri = _soup(rng, 3000)
-        nrm = meshes.face_normals(tri)
+        with np.errstate(invalid="ignore"):
+            nrm = np.nan_to_num(meshes.face_normals(tri))
         med = np.zeros((tri.shape[0], 2), np.int32)
         lo, hi = np.full(3, -25.0), np.full(3, 25.0)
+    else:
+        tri, nrm, med = meshes.curved_abdomen(freq=12)
+        lo, hi = np.array([-150, -120, -100]), np.array([150, 120, 100])
     n = 20000
     orig = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
-    # a quarter of the rays start on a triangle (as photons do after a boundary hit)
-    k = n // 4
+    k = n // 4   # a quarter of the rays start on a triangle, as photons do after a boundary hit
     pick = rng.integers(0, tri.shape[0], k)
     bc = rng.dirichlet([1, 1, 1], k)
     tt = tri[pick].reshape(k, 3, 3).astype(np.float64)
     orig[:k] = np.einsum("ki,kij->kj", bc, tt).astype(np.float32)
     d = rng.normal(size=(n, 3))
-    d[:200] = [0, 0, 1]                     # axis-aligned rays
+    d[:200] = [0, 0, 1]
     d[200:400] = [1, 0, 0]
     d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
     ref = np.full(n, -1, np.int32)
@@ -100,37 +120,64 @@ def test_bvh_query_matches_brute_force(oracle_lib, mesh):
     assert mism == 0, f"{mism} of {n} queries differ from the brute-force scan"
 
 
-def test_common_random_numbers_trajectories(oracle_lib, slab):
-    n, seed = 4000, 1234
-    t_gpu, rec_gpu = gpu_run(slab, n, seed, exit_records=n)
-    r = po.run(to_case(slab), n, rng_mode=po.RNG_PHILOX, seed=seed, exit_records=True, nthreads=0)
+@pytest.mark.parametrize("case", ["slab", "abdomen"])
+def test_common_random_numbers_trajectories(oracle_lib, slab, abdomen_small, case):
+    w = slab if case == "slab" else abdomen_small
+    n, seed = (4000, 1234) if case == "slab" else (600, 77)
+    t_gpu, rec_gpu = gpu_run(w, n, seed, exit_records=n, exact=True)
+    r = po.run(to_case(w), n, rng_mode=po.RNG_PHILOX, seed=seed, exit_records=True, nthreads=0,
+               compat=w.compat)
     same = np.all(rec_gpu.view(np.uint32) == r.exit_rec.view(np.uint32), axis=1)
     close = np.all(np.isclose(rec_gpu, r.exit_rec, rtol=1e-4, atol=1e-5), axis=1)
-    # a photon diverges only after a last-place difference of a transcendental flips a decision
-    assert close.mean() > 0.9, f"only {close.mean():.3f} of photons agree (bit-equal {same.mean():.3f})"
-    # common random numbers: aggregate tallies agree far inside the statistical error
+    # a photon diverges only after a last-place difference of a transcendental flips a decision;
+    # with the fibre source every start point and direction already carries such differences
+    # (cosf/sinf of the disk and cone sampling), so fewer trajectories stay identical there
+    need = 0.9 if case == "slab" else 0.8
+    assert close.mean() > need, f"only {close.mean():.3f} of photons agree (bit-equal {same.mean():.3f})"
     R_g = t_gpu["sft"][:, :, 0].sum() / FIX / n
     R_o = r.sft[:, :, 0].sum() / FIX / n
-    assert abs(R_g - R_o) < 0.01
+    assert abs(R_g - R_o) < 0.02
     assert t_gpu["counters"]["photons"] == n
 
 
-def test_statistical_parity(oracle_lib, slab):
-    """Independent streams, 8 batches each: region absorption, R, T and radial bins."""
-    B, n = 8, 3000
-    case = to_case(slab)
+@pytest.mark.parametrize("case", ["slab", "abdomen"])
+def test_statistical_parity_fast_mode(oracle_lib, slab, abdomen_small, case):
+    """Production kernel vs the oracle, independent streams, 8 batches each:
+    reflectance, fetal and transmitted sums, absorption per region, ring detectors
+    and the first 40 radial reflectance bins."""
+    w = slab if case == "slab" else abdomen_small
+    B, n = (8, 3000) if case == "slab" else (8, 150)
+    c = to_case(w)
     g_b, o_b = [], []
     for b in range(B):
-        t, _ = gpu_run(slab, n, seed=1000 + b)
-        r = po.run(case, n, rng_mode=po.RNG_PHILOX, seed=5000 + b)
-        for dst, sft, reg, rb in ((g_b, t["sft"], t["region"], t["rbins"]), (o_b, r.sft, r.region, r.rbins)):
-            dst.append(np.concatenate([[sft[:, :, 0].sum(), sft[:, :, 2].sum()], reg[1:],
-                                       rb[:40, 0]]) / FIX / n)
+        t, _ = gpu_run(w, n, seed=1000 + b)
+        r = po.run(c, n, rng_mode=po.RNG_PHILOX, seed=5000 + b, compat=w.compat)
+        g_b.append(np.concatenate([scalars(t["sft"], t["region"], t["det"]), t["rbins"][:40, 0]]) / FIX / n)
+        o_b.append(np.concatenate([scalars(r.sft, r.region, r.det), r.rbins[:40, 0]]) / FIX / n)
     z = z_scores(g_b, o_b)
-    scalars = z[:5]
-    assert np.all(np.abs(scalars) < 3), f"scalar tallies z = {scalars}"
-    bins = z[5:][np.isfinite(z[5:])]
-    assert np.all(np.abs(bins) < 4.5), f"radial bins max |z| = {np.abs(bins).max()}"
+    ns = 3 + (w.nmuasg.shape[0] - 1) + (0 if w.det_r is None else w.det_r.shape[0])
+    zs = z[:ns][np.isfinite(z[:ns])]
+    assert np.all(np.abs(zs) < 3), f"scalar tallies z = {z[:ns]}"
+    zb = z[ns:][np.isfinite(z[ns:])]
+    assert np.all(np.abs(zb) < 4.5), f"radial bins max |z| = {np.abs(zb).max()}"
+
+
+def test_fast_matches_reference_arithmetic_high_statistics(slab):
+    """Fast vs reference-order arithmetic on the GPU, 10 batches of 100k photons each:
+    every scalar tally within 3 sigma and the voxel absorption grid within 1% relative L2."""
+    B, n = 10, 100_000
+    a_b, b_b, va, vb = [], [], 0, 0
+    for b in range(B):
+        ta, _ = gpu_run(slab, n, seed=300 + b, exact=False)
+        tb, _ = gpu_run(slab, n, seed=700 + b, exact=True)
+        a_b.append(scalars(ta["sft"], ta["region"]) / FIX / n)
+        b_b.append(scalars(tb["sft"], tb["region"]) / FIX / n)
+        va = va + ta["vox"].astype(np.float64)
+        vb = vb + tb["vox"].astype(np.float64)
+    z = z_scores(a_b, b_b)
+    assert np.all(np.abs(z[np.isfinite(z)]) < 3), z
+    rel_l2 = np.linalg.norm(va - vb) / np.linalg.norm(vb)
+    assert rel_l2 < 0.01, rel_l2
 
 
 def test_determinism_and_split_runs(slab):
@@ -151,11 +198,10 @@ def test_determinism_and_split_runs(slab):
     assert c["counters"]["photons"] == n
 
 
-def test_fixed_point_tallies_match_oracle_bins(oracle_lib, slab):
-    """Same seed: the binned images come from the same records where trajectories agree;
-    the totals per image agree to a small fraction of the per-photon spread."""
+def test_tally_totals_match_oracle_same_seed(oracle_lib, slab):
+    """Reference arithmetic and the same seed: every image total agrees closely."""
     n, seed = 3000, 99
-    t, _ = gpu_run(slab, n, seed)
+    t, _ = gpu_run(slab, n, seed, exact=True)
     r = po.run(to_case(slab), n, rng_mode=po.RNG_PHILOX, seed=seed)
     for k, o in (("sft", r.sft), ("rtd", r.rtd), ("rz", r.rz), ("vox", r.vox)):
         tg, to = t[k].sum() / FIX / n, o.sum() / FIX / n
