@@ -127,6 +127,12 @@ int lp_set_extra_tallies(lp_ctx *ctx, const int32_t *vox_n, const float *vox_d,
  * operations (precomputed Henyey-Greenstein factors, direction-cosine scattering
  * update, vector refraction, reciprocal multiplies, FMA). */
 int lp_set_arithmetic(lp_ctx *ctx, int exact);
+/* Safety grid (no reference counterpart): a grid of at most max_cells cells over the
+ * mesh bounds holding, per cell, a lower bound of the distance to the nearest
+ * triangle, built on the device once per mesh (default 2^24 cells).  A step shorter
+ * than the bound at the photon's position cannot reach a triangle, so its
+ * nearest-triangle query is skipped without changing any result.  0 disables it. */
+int lp_set_safety_grid(lp_ctx *ctx, int64_t max_cells);
 /* Per-photon step cap (watchdog); photons that reach it are stopped and counted. */
 int lp_set_max_steps(lp_ctx *ctx, int64_t max_steps);
 /* Keep the per-photon float8 exit records of the next runs (RecordFSTxy,

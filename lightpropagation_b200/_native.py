@@ -75,6 +75,7 @@ _SIGS = {
     "lp_set_extra_tallies": ([C.c_void_p, _ip, _fp, C.c_int32, C.c_float, C.c_int32, _fp], C.c_int),
     "lp_set_max_steps": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_set_arithmetic": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_set_safety_grid": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "lp_run_async": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),

@@ -31,6 +31,8 @@ cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *ori
                          cudaStream_t s);
 cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out,
                           cudaStream_t s);
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, uint16_t *out,
+                               cudaStream_t s);
 double fma_peak_tflops(int num_sms);
 int block_size();
 }  // namespace lp
@@ -103,6 +105,13 @@ struct lp_ctx {
     DevBuf<Medium> media;
     DevBuf<unsigned long long> sft, rtd, rz, vox, rbins, region, det, counters, work;
     DevBuf<float> exit_rec;
+    // safety grid (lp_set_safety_grid)
+    int64_t grid_max_cells = int64_t(1) << 24;
+    bool grid_dirty = true;
+    DevBuf<uint16_t> safe;
+    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0;
+    int32_t g_n[3] = {0, 0, 0};
+    float grid_ms = 0;
     // host copies of tallies
     std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
     float last_ms = 0.0f;
@@ -258,6 +267,8 @@ int upload_media(lp_ctx *c)
     return LP_OK;
 }
 
+int build_safety_grid(lp_ctx *c);
+
 int upload(lp_ctx *c)
 {
     if (!c->have_mesh || !c->have_media || !c->have_source || !c->have_grid)
@@ -278,6 +289,10 @@ int upload(lp_ctx *c)
         c->tally_dirty = false;
     }
     if (c->exit_cap > 0) LP_CUDA(c, c->exit_rec.ensure((size_t)c->exit_cap * 8));
+    if (c->grid_dirty) {
+        r = build_safety_grid(c);
+        if (r) return r;
+    }
     return LP_OK;
 }
 
@@ -366,6 +381,72 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.exit_rec = c->exit_cap > 0 ? c->exit_rec.p : nullptr;
     P.exit_cap = c->exit_cap;
     P.work = c->work.p;
+    P.safe_grid = (c->grid_max_cells > 0 && c->safe.p && !c->grid_dirty) ? c->safe.p : nullptr;
+    P.g_ox = c->g_origin[0];
+    P.g_oy = c->g_origin[1];
+    P.g_oz = c->g_origin[2];
+    P.g_inv_h = c->g_h > 0 ? 1.0f / c->g_h : 0.0f;
+    P.g_unit = c->g_unit;
+    P.g_nx = c->g_n[0];
+    P.g_ny = c->g_n[1];
+    P.g_nz = c->g_n[2];
+}
+
+// Safety grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
+// the grid has at most grid_max_cells cells; values in units of h / 256.
+int build_safety_grid(lp_ctx *c)
+{
+    c->grid_dirty = false;
+    if (c->grid_max_cells <= 0 || c->n_tri == 0) {
+        c->safe.release();
+        return LP_OK;
+    }
+    const lp::Bvh &b = c->bvh;
+    double ext[3], vol = 1.0, scale = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        ext[a] = std::max((double)b.hi[a] - b.lo[a], 1e-6);
+        vol *= ext[a];
+        scale = std::max({scale, ext[a], std::fabs((double)b.lo[a]), std::fabs((double)b.hi[a])});
+    }
+    double h = std::cbrt(vol / (double)c->grid_max_cells);
+    h = std::max(h, 1e-6 * scale);
+    int64_t cells = 0;
+    for (int it = 0; it < 200; ++it) {
+        cells = 1;
+        for (int a = 0; a < 3; ++a) {
+            c->g_n[a] = (int32_t)std::ceil(ext[a] / h) + 2;
+            cells *= c->g_n[a];
+        }
+        if (cells <= c->grid_max_cells) break;
+        h *= 1.05;
+    }
+    if (cells > c->grid_max_cells) return fail(c, LP_ERR_RANGE, "safety grid: cannot fit %lld cells", (long long)cells);
+    c->g_h = (float)h;
+    c->g_unit = (float)(h / 256.0);
+    for (int a = 0; a < 3; ++a) c->g_origin[a] = (float)(b.lo[a] - h);
+    LP_CUDA(c, c->safe.ensure((size_t)cells));
+    KParams P;
+    std::memset(&P, 0, sizeof P);
+    P.node_a = c->node_a.p; P.node_b = c->node_b.p; P.node_c = c->node_c.p; P.node_d = c->node_d.p;
+    P.tri_a = c->tri_a.p; P.tri_b = c->tri_b.p; P.tri_c = c->tri_c.p;
+    P.g_ox = c->g_origin[0]; P.g_oy = c->g_origin[1]; P.g_oz = c->g_origin[2];
+    P.g_nx = c->g_n[0]; P.g_ny = c->g_n[1]; P.g_nz = c->g_n[2];
+    P.g_unit = c->g_unit;
+    // eps: far above the few-ulp overreach of the ray/triangle test at this scale
+    const float eps = (float)(1e-4 * scale);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->stream);
+    cudaError_t e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(250.0 * h),
+                                           c->safe.p, c->stream);
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&c->grid_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(c, e, "safety grid");
+    return LP_OK;
 }
 
 // shared-memory staging: as many top BVH levels and leading triangles as fit the budget
@@ -424,6 +505,7 @@ void lp_destroy(lp_ctx *c)
     c->sft.release(); c->rtd.release(); c->rz.release(); c->vox.release(); c->rbins.release();
     c->region.release(); c->det.release(); c->counters.release(); c->work.release();
     c->exit_rec.release();
+    c->safe.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -457,6 +539,7 @@ int lp_set_mesh(lp_ctx *c, int64_t n_tri, const float *tri, const float *nrm, co
     for (int64_t i = 0; i < 2 * n_tri; ++i) c->max_region = std::max(c->max_region, med[i]);
     c->have_mesh = true;
     c->mesh_dirty = true;
+    c->grid_dirty = true;
     return LP_OK;
 }
 
@@ -557,6 +640,15 @@ int lp_set_arithmetic(lp_ctx *c, int exact)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_arithmetic: ctx is NULL");
     c->exact = exact != 0;
+    return LP_OK;
+}
+
+int lp_set_safety_grid(lp_ctx *c, int64_t max_cells)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_safety_grid: ctx is NULL");
+    if (max_cells < 0 || max_cells > (int64_t(1) << 28)) return fail(c, LP_ERR_RANGE, "lp_set_safety_grid: %lld cells", (long long)max_cells);
+    c->grid_max_cells = max_cells;
+    c->grid_dirty = true;
     return LP_OK;
 }
 

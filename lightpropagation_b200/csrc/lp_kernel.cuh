@@ -66,9 +66,26 @@ struct KParams {
     float det_lo[kMaxDet], det_hi[kMaxDet];
     float *exit_rec;
     int64_t exit_cap;
+    // safety grid: per cell a lower bound of the distance from any point of the cell to
+    // the nearest triangle, in units of g_unit (0 = unknown / near a surface)
+    const uint16_t *safe_grid;
+    float g_ox, g_oy, g_oz, g_inv_h, g_unit;
+    int32_t g_nx, g_ny, g_nz;
     // scratch: photon work counter
     unsigned long long *work;
 };
+
+// Conservative distance from p to the nearest triangle, read from the safety grid.
+__device__ __forceinline__ float safe_distance(const KParams &P, float px, float py, float pz)
+{
+    if (!P.safe_grid) return 0.0f;
+    const int ix = (int)floorf((px - P.g_ox) * P.g_inv_h);
+    const int iy = (int)floorf((py - P.g_oy) * P.g_inv_h);
+    const int iz = (int)floorf((pz - P.g_oz) * P.g_inv_h);
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= P.g_nx || iy >= P.g_ny || iz >= P.g_nz) return 0.0f;
+    const unsigned short q = __ldg(P.safe_grid + ((int64_t)iz * P.g_ny + iy) * P.g_nx + ix);
+    return (float)q * P.g_unit;
+}
 
 // ----------------------------------------------------------------- Philox4x32-10
 __device__ __forceinline__ void philox4x32_10(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t &c3,

@@ -1,0 +1,135 @@
+// lp_safety.cu -- safety-distance grid over the mesh, built once per mesh on the GPU.
+//
+// Cell value = a lower bound, in units of `unit`, of the distance from ANY point of the
+// cell to the nearest triangle: (exact distance from the cell centre) - (half cell
+// diagonal) - eps, rounded down.  eps covers the rounding of the reference's
+// ray/triangle test, which can accept intersection points a few ulp outside a
+// triangle.  A transport step shorter than this bound cannot reach any triangle, so
+// the bounded nearest-hit query would return "no hit": the kernel skips it and the
+// result is unchanged.
+#include <algorithm>
+
+#include "lp_kernel.cuh"
+
+namespace lp {
+
+// Squared distance from p to the triangle (a, a + ab, a + ac): closest point by Voronoi
+// regions of the vertices, edges and face (Ericson, Real-Time Collision Detection, 2005).
+__device__ __forceinline__ float point_triangle_dist2(V3 p, V3 a, V3 ab, V3 ac)
+{
+    const V3 ap = sub3(p, a);
+    const float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    V3 q;
+    if (d1 <= 0.0f && d2 <= 0.0f) {
+        q = a;
+    } else {
+        const V3 b = add3(a, ab), c = add3(a, ac);
+        const V3 bp = sub3(p, b);
+        const float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+        const V3 cp = sub3(p, c);
+        const float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+        const float vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+        if (d3 >= 0.0f && d4 <= d3) {
+            q = b;
+        } else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+            q = add3(a, scl3(d1 / (d1 - d3), ab));
+        } else if (d6 >= 0.0f && d5 <= d6) {
+            q = c;
+        } else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+            q = add3(a, scl3(d2 / (d2 - d6), ac));
+        } else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+            const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+            q = add3(b, scl3(w, sub3(c, b)));
+        } else {
+            const float den = 1.0f / (va + vb + vc);
+            q = add3(a, add3(scl3(vb * den, ab), scl3(vc * den, ac)));
+        }
+    }
+    const V3 d = sub3(p, q);
+    return dot3(d, d);
+}
+
+__device__ __forceinline__ float box_dist2(float lo_x, float hi_x, float lo_y, float hi_y, float lo_z, float hi_z,
+                                           V3 p)
+{
+    const float dx = fmaxf(fmaxf(lo_x - p.x, 0.0f), p.x - hi_x);
+    const float dy = fmaxf(fmaxf(lo_y - p.y, 0.0f), p.y - hi_y);
+    const float dz = fmaxf(fmaxf(lo_z - p.z, 0.0f), p.z - hi_z);
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// Distance^2 from p to the nearest triangle, or cap2 if none is closer.
+__device__ float nearest_dist2(const KParams &P, V3 p, float cap2)
+{
+    float best = cap2;
+    int stack[kStackDepth];
+    int sp = 0, node = 0;
+    for (;;) {
+        const float4 a = __ldg(P.node_a + node), b = __ldg(P.node_b + node), c = __ldg(P.node_c + node);
+        const int4 d = __ldg(P.node_d + node);
+        const float d0 = box_dist2(a.x, a.y, a.z, a.w, c.x, c.y, p);
+        const float d1 = box_dist2(b.x, b.y, b.z, b.w, c.z, c.w, p);
+        int next[2];
+        float nd[2];
+        int k = 0;
+        const int ref[2] = {d.x, d.y};
+        const float dd[2] = {d0, d1};
+        for (int s = 0; s < 2; ++s) {
+            if (!(dd[s] < best)) continue;
+            if (ref[s] < 0) {
+                const int e = ~ref[s], f = e >> 3, cnt = (e & 7) + 1;
+                for (int j = f; j < f + cnt; ++j) {
+                    const float4 ta = __ldg(P.tri_a + j), tb = __ldg(P.tri_b + j), tc = __ldg(P.tri_c + j);
+                    const float q = point_triangle_dist2(p, v3(ta.x, ta.y, ta.z), v3(ta.w, tb.x, tb.y),
+                                                         v3(tb.z, tb.w, tc.x));
+                    best = fminf(best, q);
+                }
+            } else {
+                next[k] = ref[s];
+                nd[k] = dd[s];
+                ++k;
+            }
+        }
+        if (k == 2) {
+            const bool f0 = nd[0] <= nd[1];
+            if (sp < kStackDepth) stack[sp++] = f0 ? next[1] : next[0];
+            node = f0 ? next[0] : next[1];
+        } else if (k == 1) {
+            node = next[0];
+        } else {
+            // pop, skipping subtrees that the shrinking best has ruled out is left to the child test
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return best;
+}
+
+__global__ void __launch_bounds__(256) safety_grid_kernel(const __grid_constant__ KParams P, float h,
+                                                          float half_diag, float eps, float cap,
+                                                          uint16_t *out)
+{
+    const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
+    const float inv_unit = 1.0f / P.g_unit;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i % P.g_nx);
+        const int iy = (int)((i / P.g_nx) % P.g_ny);
+        const int iz = (int)(i / ((int64_t)P.g_nx * P.g_ny));
+        const V3 c = v3(P.g_ox + (ix + 0.5f) * h, P.g_oy + (iy + 0.5f) * h, P.g_oz + (iz + 0.5f) * h);
+        const float d = sqrtf(nearest_dist2(P, c, cap * cap));
+        const float safe = (d - half_diag - eps) * 0.9999f;
+        float q = safe > 0.0f ? floorf(safe * inv_unit) : 0.0f;
+        out[i] = (uint16_t)fminf(q, 65535.0f);
+    }
+}
+
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, uint16_t *out,
+                               cudaStream_t s)
+{
+    const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    safety_grid_kernel<<<std::max(grid, 1), 256, 0, s>>>(P, h, half_diag, eps, cap, out);
+    return cudaGetLastError();
+}
+
+}  // namespace lp

@@ -49,7 +49,7 @@ enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2 };
 enum : uint32_t { EXIT_NONE = 0, EXIT_SURF = 1, EXIT_SURF_FETAL = 2, EXIT_TRANS = 3 };
 
 struct Counters {
-    uint32_t scatter, boundary, query, roulette, rz_drop, vox_drop;
+    uint32_t scatter, boundary, query, roulette, rz_drop, vox_drop, skip;
 };
 
 template <bool Exact>
@@ -113,14 +113,16 @@ __device__ __forceinline__ V3 scatter_direction(V3 v, const Medium &m, float xt,
         const V3 rot_theta = norm3(rotate(v, e_rot, cosTheta, sinTheta));
         return norm3(rotate(rot_theta, v, cosPsi, sinPsi));
     } else {
-        // direction-cosine update (Wang, Jacques & Zheng, MCML 1995)
+        // direction-cosine update (Wang, Jacques & Zheng, MCML 1995).  1 - uz^2 is taken
+        // as ux^2 + uy^2 (|v| = 1), which keeps its precision near the z axis where the
+        // difference form cancels; the axial case scatters about z with uz' = sign(uz) cos.
         const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
         float sinPsi, cosPsi;
         sincospif(2.0f * xp, &sinPsi, &cosPsi);
         V3 r;
-        const float uz2 = 1.0f - v.z * v.z;
-        if (uz2 < 1e-10f) {
-            r = v3(sinTheta * cosPsi, sinTheta * sinPsi, copysignf(cosTheta, v.z));
+        const float uz2 = v.x * v.x + v.y * v.y;
+        if (uz2 < 1e-20f) {
+            r = v3(sinTheta * cosPsi, sinTheta * sinPsi, v.z > 0.0f ? cosTheta : -cosTheta);
         } else {
             const float it = rsqrtf(uz2);
             const float temp = uz2 * it;  // sqrt(1 - uz^2)
@@ -281,9 +283,17 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         }
     }
     float thit;
+    int tri;
     const V3 p = v3(ph.px, ph.py, ph.pz), v = v3(ph.vx, ph.vy, ph.vz);
-    const int tri = query_nearest(M, p, v, ph.refTri, m.ambient ? kNoHit : step, thit);
-    cnt.query++;
+    if (!m.ambient && step < safe_distance(P, p.x, p.y, p.z)) {
+        // no triangle within the step: the bounded query would return "no hit"
+        tri = -1;
+        thit = kNoHit;
+        cnt.skip++;
+    } else {
+        tri = query_nearest(M, p, v, ph.refTri, m.ambient ? kNoHit : step, thit);
+        cnt.query++;
+    }
     if (m.ambient) step = thit;
     const bool boundary = (tri >= 0) ? (thit <= step) : (kNoHit <= step);
     if (boundary) {
@@ -562,6 +572,9 @@ __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_const
         unsigned long long x = photons;
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0 && x) atomicAdd(s_cnt + 8, x);
+        x = cnt.skip;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0 && x) atomicAdd(s_cnt + 10, x);
     }
     __syncthreads();
     if (threadIdx.x < 16 && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);

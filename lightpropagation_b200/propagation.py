@@ -108,6 +108,10 @@ class Simulation:
         """exact=True: the reference kernel's operation order; False (default): fast."""
         self._ck(self._L.lp_set_arithmetic(self._h, 1 if exact else 0))
 
+    def set_safety_grid(self, max_cells: int):
+        """Cells of the query-skipping safety grid (0 disables it; results are unchanged)."""
+        self._ck(self._L.lp_set_safety_grid(self._h, int(max_cells)))
+
     def set_max_steps(self, n: int):
         self._ck(self._L.lp_set_max_steps(self._h, int(n)))
 

@@ -180,6 +180,30 @@ def test_fast_matches_reference_arithmetic_high_statistics(slab):
     assert rel_l2 < 0.01, rel_l2
 
 
+@pytest.mark.parametrize("case,exact", [("slab", False), ("abdomen", False), ("abdomen", True)])
+def test_safety_grid_changes_nothing(slab, case, exact):
+    """Skipping queries whose step cannot reach a triangle must leave every tally
+    bit-identical; the grid must also actually skip queries."""
+    w = slab if case == "slab" else workloads.curved_abdomen(freq=20)
+    n = 20000
+    out = []
+    for cells in (0, 1 << 22):
+        with Simulation(0) as s:
+            w.apply(s, seed=31)
+            s.set_arithmetic(exact)
+            s.set_safety_grid(cells)
+            s.zero()
+            s.run(n)
+            out.append(s.tallies())
+    a, b = out
+    for k in ("sft", "rtd", "rz", "vox", "rbins", "region", "det"):
+        assert np.array_equal(a[k], b[k]), k
+    ca, cb = a["counters"], b["counters"]
+    assert ca["scatter"] == cb["scatter"] and ca["boundary"] == cb["boundary"]
+    assert ca["safe_skip"] == 0 and cb["safe_skip"] > 0.3 * cb["scatter"]
+    assert cb["query"] + cb["safe_skip"] == ca["query"]
+
+
 def test_determinism_and_split_runs(slab):
     n = 6000
     a, _ = gpu_run(slab, n, seed=7)
