@@ -224,7 +224,11 @@ def reference_arm(args, w):
 
 # ------------------------------------------------------------------ our arm
 def fp32_flops_per_photon(c, n):
-    es, eb, eq = c["scatter"] / n, c["boundary"] / n, c["query"] / n
+    """Algorithmic FP32 work per photon.  E_q counts the queries of the reference's
+    algorithm (one per loop iteration, FindTriangleInPath at .cl:1379), not the ones the
+    kernel executes after safety-grid skips."""
+    es, eb = c["scatter"] / n, c["boundary"] / n
+    eq = es + eb
     return 64 * es + 48 * eb + 40 * eq, es, eb, eq
 
 
@@ -349,7 +353,10 @@ def ours_arm(args, w):
             "frac": achieved / peak if peak else None,
             "traffic": (tpp * n) if tpp is not None else None,
             "peak_source": "FP32 FMA peak measured in-run by lp_fp32_peak (MEASURED_PEAKS.json has no FP32 figure)",
-            "flops_per_photon": F, "events_per_photon": {"scatter": es, "boundary": eb, "query": eq}}
+            "flops_per_photon": F,
+            "events_per_photon": {"scatter": es, "boundary": eb, "query": eq,
+                                  "query_executed": counters["query"] / per_launch_photons,
+                                  "query_skipped_by_safety_grid": counters["safe_skip"] / per_launch_photons}}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

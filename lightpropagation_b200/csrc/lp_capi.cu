@@ -438,7 +438,7 @@ int build_safety_grid(lp_ctx *c)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c->stream);
-    cudaError_t e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(250.0 * h),
+    cudaError_t e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h),
                                            c->safe.p, c->stream);
     cudaEventRecord(e1, c->stream);
     cudaEventSynchronize(e1);
