@@ -185,6 +185,48 @@ int lp_get_device_tallies(lp_ctx *ctx, lp_device_tallies *out);
  * dependent-FMA kernel: the roofline denominator of the transport kernel. */
 int lp_fp32_peak(int device, double *tflops);
 
+/* --- transport without device allocation ------------------------------------- */
+/* No counterpart in the reference.  For callers that must not allocate device memory
+ * through this library: code running while a stream is being captured into a CUDA
+ * graph, or a host application whose device memory comes from its own pool or arena
+ * with a fixed budget.  lp_run_noalloc traces photons [first, first + n_photons) with
+ * the reference-arithmetic transport kernel and never calls cudaMalloc or cudaFree.
+ * Its scratch (photon counter, event counters, media table and a small BVH built on
+ * the device from the mesh arrays) lives in one static device array of
+ * LP_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
+ *   - mesh arrays are DEVICE pointers in the reference layouts (tri 9 floats, nrm 3
+ *     floats, med 2 ints per triangle); region ids must be < n_media;
+ *   - nmuasg is a HOST pointer (n, mua, mus, g per region), copied into kernel params;
+ *   - sft, rtd, rz, region are DEVICE outputs in the lp_tallies layouts (sizes as
+ *     lp_get_geometry reports for the same dimensions and grid); results are ADDED to
+ *     them, so zero them first; counters (16 uint64) is optional;
+ *   - sizes beyond LP_NOALLOC_MAX_TRI triangles or LP_NOALLOC_MAX_MEDIA regions are
+ *     rejected with LP_ERR_RANGE.
+ * The call is asynchronous on `stream` (a cudaStream_t, NULL for the default stream).
+ * The first call on a device looks up the scratch address; make that first call
+ * before any stream capture.  All calls share the one scratch array, so calls that
+ * overlap on the GPU race: serialise them on one stream. */
+#define LP_NOALLOC_MAX_TRI 4096
+#define LP_NOALLOC_MAX_MEDIA 64
+#define LP_NOALLOC_SCRATCH_BYTES (384 * 1024)
+typedef struct lp_noalloc_args {
+    const float *tri, *nrm;
+    const int32_t *med;
+    int64_t n_tri;
+    const float *nmuasg;
+    int32_t n_media;
+    float p_start[3], v_start[3], ep0xyz[12];
+    float fiber_radius, fiber_cos_max;   /* fibre source; 0 and 1 for the pencil beam */
+    float dimensions[3], det_grid[6];
+    int32_t fetal_id;
+    float chance, w_threshold, factor;
+    uint64_t seed;
+    uint32_t compat;
+    int64_t first, n_photons;
+    uint64_t *sft, *rtd, *rz, *region, *counters;
+} lp_noalloc_args;
+int lp_run_noalloc(const lp_noalloc_args *args, void *stream);
+
 /* --- verification entry points ---------------------------------------------- */
 /* Nearest-triangle queries through the device BVH for n rays (FindTriangleInPath,
  * MCLightPropagation.cl:1037-1093): origins/dirs 3 floats per ray, ref_tri the

@@ -52,6 +52,22 @@ class DeviceTallies(C.Structure):
                                   "n_counters")] + [("stream", C.c_void_p)]
 
 
+class NoAllocArgs(C.Structure):
+    """lp_noalloc_args: mesh as device pointers, media on the host, outputs on the device."""
+    _fields_ = [("tri", C.c_void_p), ("nrm", C.c_void_p), ("med", C.c_void_p), ("n_tri", C.c_int64),
+                ("nmuasg", _fp), ("n_media", C.c_int32),
+                ("p_start", C.c_float * 3), ("v_start", C.c_float * 3), ("ep0xyz", C.c_float * 12),
+                ("fiber_radius", C.c_float), ("fiber_cos_max", C.c_float),
+                ("dimensions", C.c_float * 3), ("det_grid", C.c_float * 6), ("fetal_id", C.c_int32),
+                ("chance", C.c_float), ("w_threshold", C.c_float), ("factor", C.c_float),
+                ("seed", C.c_uint64), ("compat", C.c_uint32), ("first", C.c_int64), ("n_photons", C.c_int64),
+                ("sft", C.c_void_p), ("rtd", C.c_void_p), ("rz", C.c_void_p), ("region", C.c_void_p),
+                ("counters", C.c_void_p)]
+
+
+NOALLOC_MAX_TRI, NOALLOC_MAX_MEDIA = 4096, 64
+
+
 class LPError(RuntimeError):
     """Raised when a liblpcuda call returns a non-zero status."""
 
@@ -90,6 +106,7 @@ _SIGS = {
     "lp_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "lp_get_device_tallies": ([C.c_void_p, C.POINTER(DeviceTallies)], C.c_int),
     "lp_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "lp_run_noalloc": ([C.POINTER(NoAllocArgs), C.c_void_p], C.c_int),
 }
 
 EXPORTED = sorted(_SIGS)

@@ -462,6 +462,12 @@ void smem_plan(const lp_ctx *c, int budget, int &nodes_smem, int &tris_smem)
 
 }  // namespace
 
+// helpers shared with lp_noalloc.cu
+namespace lp {
+void set_thread_error(const char *msg) { g_thread_error = msg; }
+float rspecular_of(const float *nmuasg, int n_media) { return rspecular(nmuasg, n_media); }
+}  // namespace lp
+
 // ============================================================ C ABI
 extern "C" {
 
