@@ -1,0 +1,109 @@
+"""Photon-range sharding across ranks, and the one exchange step: a sum of tallies.
+
+Photons are independent histories.  Rank r of W traces the contiguous photon-index
+range ``photon_range(n, r, W, first)`` under the same Philox key, so the ranks together
+trace exactly the photons that one GPU traces for ``[first, first + n)``: photon i draws
+its random numbers from counter (i, event, stream) whichever rank runs it.  Every tally
+is a uint64 fixed-point sum (2^32 per unit weight), and integer addition is associative
+and commutative, so the tallies summed over ranks equal the single-GPU tallies bit for
+bit.  That sum is the path's only collective: one all-reduce of one flat int64 buffer
+per launch (NCCL over NVLink on GPUs, gloo on CPU for tests).  uint64 values travel as
+int64; two's-complement addition wraps exactly like uint64 addition.
+
+This replaces nothing in the reference, which runs on one OpenCL device
+(CalculatePropagation.cpp:1389-1759); the photon loop it splits into 6400-photon
+launches is split here across ranks instead.
+"""
+from __future__ import annotations
+
+from typing import Dict, Iterable, List, Optional, Tuple
+
+import numpy as np
+
+TALLY_KEYS = ("sft", "rtd", "rz", "vox", "rbins", "region", "det")
+
+
+def photon_range(n: int, rank: int, world: int, first: int = 0) -> Tuple[int, int]:
+    """(first index, count) of rank's share of photons [first, first + n).  Shares are
+    contiguous, in rank order, and differ in size by at most one photon."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of world {world}")
+    if n < 0 or first < 0:
+        raise ValueError("negative photon range")
+    base, extra = divmod(int(n), int(world))
+    start = first + rank * base + min(rank, extra)
+    return start, base + (1 if rank < extra else 0)
+
+
+def allreduce_flat(tensors: List["object"], group=None) -> None:
+    """Sum int64 tensors over the process group in place with ONE all-reduce: pack them
+    into a flat buffer on their device, reduce it, unpack."""
+    import torch
+    import torch.distributed as dist
+    if not tensors:
+        return
+    for t in tensors:
+        if t.dtype != torch.int64:
+            raise TypeError("tallies are reduced as int64")
+    flat = torch.cat([t.reshape(-1) for t in tensors])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    off = 0
+    for t in tensors:
+        k = t.numel()
+        t.view(-1).copy_(flat[off:off + k])
+        off += k
+
+
+def reduce_host_tallies(tallies: Dict[str, object], group=None) -> Dict[str, object]:
+    """Sum host tallies (numpy uint64 arrays and the ``counters`` dict) over the group.
+    Returns a new dict with the same keys and shapes; the inputs are not modified."""
+    import torch
+    keys = [k for k in TALLY_KEYS if k in tallies]
+    arrays = [np.ascontiguousarray(tallies[k], np.uint64) for k in keys]
+    names = sorted(tallies["counters"]) if "counters" in tallies else []
+    cnt = np.array([tallies["counters"][k] for k in names], np.uint64)
+    ts = [torch.from_numpy(a.view(np.int64).copy()) for a in arrays + [cnt]]
+    allreduce_flat(ts, group)
+    out = {k: t.numpy().view(np.uint64).reshape(a.shape) for k, a, t in zip(keys, arrays, ts)}
+    if names:
+        out["counters"] = {k: int(v) for k, v in zip(names, ts[-1].numpy().view(np.uint64))}
+    return out
+
+
+class _DeviceArray:
+    """A raw device pointer seen by torch through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<i8", "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def device_tally_tensors(sim, device: int) -> List["object"]:
+    """The context's device tally buffers (and counters) as int64 torch tensors that alias
+    them; valid until the tally layout changes (lp_set_tally_grid / lp_set_extra_tallies)."""
+    import torch
+    d = sim.device_tallies()
+    out = []
+    for name in TALLY_KEYS + ("counters",):
+        cnt = getattr(d, "n_" + name)
+        if cnt > 0:
+            out.append(torch.as_tensor(_DeviceArray(getattr(d, name), cnt), device=f"cuda:{device}"))
+    return out
+
+
+def run_sharded(sim, n: int, first: int = 0, group=None, device: Optional[int] = None,
+                tensors: Optional[Iterable["object"]] = None) -> None:
+    """Trace this rank's share of photons [first, first + n) on its GPU into the zeroed
+    tallies of `sim`, then sum the device tallies over the group in place (NCCL).
+    Afterwards every rank's ``sim.tallies()`` holds the tallies of all n photons.
+    `tensors` may pass the aliases from device_tally_tensors to skip re-querying them."""
+    import torch
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    f, k = photon_range(n, rank, world, first)
+    sim.run(k, f)
+    dev = torch.cuda.current_device() if device is None else device
+    ts = list(tensors) if tensors is not None else device_tally_tensors(sim, dev)
+    with torch.cuda.device(dev):
+        allreduce_flat(ts, group)
+        torch.cuda.current_stream().synchronize()
