@@ -3,11 +3,18 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-A step is one pass of the hot path over one batch: ``--photons`` photons of the
-workload traced through the mesh, tallies zeroed before and complete after.
-Photons are sharded by index range across ranks (weak scaling: every rank traces
-the same number of photons per step); the integer tallies are summed over ranks
-with one NCCL all-reduce per step, inside the timed region.
+A step is one pass of the hot path over one batch per case: ``--photons`` photons
+of each case traced through the mesh, tallies zeroed before and complete after.
+The default workload is the curved-mesh abdomen (202,500 triangles, fibre source,
+six ring detectors) at 660 nm and at 940 nm, so a step is two launches on one
+mesh with the media table switched between them; ``--workload plain_slab`` is the
+small 3-layer slab.  Photons are sharded by index range across ranks (weak
+scaling: every rank traces the same number of photons per step); the integer
+tallies are summed over ranks with one NCCL all-reduce per launch, inside the
+timed region.
+
+detector_error  relative standard error of every ring detector's signal after one
+       launch, and the photon count that brings the farthest ring to 1%.
 
 value  photons/s of the whole job from CUDA-event device time (inputs resident),
        max over ranks; an L2-sized buffer is rewritten between timed steps.
@@ -49,12 +56,32 @@ def env_int(k, d):
         return d
 
 
-def load_workload(name, photons):
+def load_cases(name, photons):
+    """The workloads one step traces, in order.  ``curved_abdomen`` (the default) is the
+    curved-mesh abdomen at 660 nm and at 940 nm: one mesh, two optical-property tables,
+    a batch of photons at each wavelength per step."""
+    import dataclasses
     from lightpropagation_b200 import workloads
-    w = workloads.WORKLOADS[name]()
-    if photons:
-        w.n_photons = int(photons)
-    return w
+    if name == "curved_abdomen":
+        w = workloads.curved_abdomen(wavelength=660)
+        nm940 = np.array(workloads.ABDOMEN_MEDIA[940], np.float32)
+        cases = [w, dataclasses.replace(w, nmuasg=nm940, name=w.name.replace("660nm", "940nm"))]
+    else:
+        cases = [workloads.WORKLOADS[name]()]
+    for c in cases:
+        if photons:
+            c.n_photons = int(photons)
+    return cases
+
+
+def ring_rse(det, n):
+    """Relative standard error of each ring detector's mean signal per photon, from the
+    fixed-point sums (sum w, sum w^2) over n photons."""
+    s = det[:, 0].astype(np.float64) / 2.0 ** 32
+    s2 = det[:, 1].astype(np.float64) / 2.0 ** 32
+    var = np.maximum(s2 - s * s / n, 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(s > 0, np.sqrt(var) / s, np.inf)
 
 
 # ------------------------------------------------------------------ clocks
@@ -188,7 +215,30 @@ def bin_exit_records(rec, g, dg):
     return sft, rtd
 
 
-def reference_arm(args, w):
+def reference_sample_size(cases, threads, seconds):
+    """Photons per case for a reference sample of about `seconds` of host time."""
+    dt = sum(run_reference_sample(c, threads, threads)[0] for c in cases)
+    per_photon = dt / (threads * len(cases))
+    return int(max(threads, min(cases[0].n_photons, seconds / len(cases) / max(per_photon, 1e-9))))
+
+
+def reference_sample(cases, n, threads):
+    """n photons of every case through the reference kernel: (seconds, photons)."""
+    tot_t, tot_n = 0.0, 0
+    for c in cases:
+        t, k = run_reference_sample(c, n, threads)
+        tot_t += t
+        tot_n += k
+    return tot_t, tot_n
+
+
+def workload_label(args, cases):
+    if len(cases) == 1:
+        return cases[0].name
+    return f"{args.workload}: " + " + ".join(c.name for c in cases)
+
+
+def reference_arm(args, cases):
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
@@ -197,26 +247,25 @@ def reference_arm(args, w):
     if L is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
-    # calibrate a bounded sample (a few seconds per step)
-    dt, n0 = run_reference_sample(w, threads, threads)
-    per_photon = dt / n0
-    n = int(max(threads, min(w.n_photons, 3.0 / max(per_photon, 1e-9))))
+    n = reference_sample_size(cases, threads, 6.0)       # a bounded sample, a few seconds per step
     for _ in range(args.warmup):
-        run_reference_sample(w, max(threads, n // 4), threads)
+        reference_sample(cases, max(threads, n // 8), threads)
     tot_t, tot_n = 0.0, 0
     for _ in range(args.steps):
-        t, k = run_reference_sample(w, n, threads)
+        t, k = reference_sample(cases, n, threads)
         tot_t += t
         tot_n += k
     v = tot_n / tot_t
+    label = workload_label(args, cases)
     line = {"metric": METRIC, "value": v, "unit": "photons/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": w.name, "photons_per_step": n, "triangles": int(w.n_tri),
+            "config": {"workload": label, "photons_per_step": n * len(cases), "triangles": int(cases[0].n_tri),
                        "parallelism": f"{threads} host threads"},
             "cpu_baseline": {"value": v, "unit": "photons/s", "cores": threads, "kind": "reference",
-                             "sample": f"{n} photons per step of {w.name} (reference kernel source compiled for "
-                                       f"the CPU + host binning)"},
+                             "sample": f"{n} photons of each of {len(cases)} case(s) per step of {label}: the "
+                                       f"reference kernel source compiled for the CPU (oracle/_ref, pencil beam "
+                                       f"source, brute-force triangle search) + ExecKernel's host binning"},
             "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -232,17 +281,20 @@ def fp32_flops_per_photon(c, n):
     return 64 * es + 48 * eb + 40 * eq, es, eb, eq
 
 
-def traffic_per_photon(workload):
-    """DRAM bytes per photon of the transport kernel from the committed ncu summary."""
+def traffic_of(workload):
+    """DRAM bytes of one transport launch and that launch's photon count, from the
+    committed ncu summary (dram__bytes_read.sum + dram__bytes_write.sum)."""
     path = os.path.join(ROOT, "profiles", f"transport_kernel_{workload}.md")
     if not os.path.isfile(path):
-        return None
+        return None, None
     import re
-    m = re.search(r"dram_bytes_per_photon:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
+    text = open(path).read()
+    b = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    p = re.search(r"dram_bytes_launch_photons:\s*([0-9.eE+]+)", text)
+    return (float(b.group(1)) if b else None), (int(float(p.group(1))) if p else None)
 
 
-def ours_arm(args, w):
+def ours_arm(args, cases):
     import torch
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
@@ -252,8 +304,9 @@ def ours_arm(args, w):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    from lightpropagation_b200 import Simulation
+    from lightpropagation_b200 import Simulation, sharding
     from lightpropagation_b200.propagation import fp32_peak_tflops
+    w, ncase = cases[0], len(cases)
     n = w.n_photons
     sim = Simulation(local)
     w.apply(sim, seed=0x4C50)
@@ -261,31 +314,34 @@ def ours_arm(args, w):
 
     red = []
     if dist is not None:
-        sim.run(0)
-        d = sim.device_tallies()
+        sim.run(0)                      # allocates the tallies; the aliases stay valid
+        red = sharding.device_tally_tensors(sim, local)
 
-        class _CA:
-            def __init__(self, ptr, cnt):
-                self.__cuda_array_interface__ = {"shape": (cnt,), "typestr": "<i8", "data": (ptr, False),
-                                                 "version": 3}
-        for name in ("sft", "rtd", "rz", "vox", "rbins", "region", "det", "counters"):
-            cnt = getattr(d, "n_" + name)
-            if cnt > 0:
-                red.append(torch.as_tensor(_CA(getattr(d, name), cnt), device=f"cuda:{local}"))
+    kernel_ms = []          # per timed launch: (case index, device ms)
 
-    def step(i):
-        sim.zero()
-        first = (i * world + rank) * n
-        sim.run(n, first)
-        ms = sim.kernel_ms()
-        if dist is not None:
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record()
-            for t in red:
-                dist.all_reduce(t)
-            ev1.record()
-            ev1.synchronize()
-            ms += ev0.elapsed_time(ev1)
+    def step(i, keep=None):
+        """One step: a batch of n photons of every case.  Returns device ms (kernels +
+        all-reduce).  `keep` collects each case's tallies after its batch."""
+        ms = 0.0
+        for j, c in enumerate(cases):
+            if ncase > 1:
+                sim.set_media(c.nmuasg)
+            sim.zero()
+            first, count = sharding.photon_range(n * world, rank, world, (i * ncase + j) * n * world)
+            sim.run(count, first)
+            k = sim.kernel_ms()
+            ms += k
+            if keep is not None:
+                kernel_ms.append((j, k))
+            if dist is not None:
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record()
+                sharding.allreduce_flat(red)
+                ev1.record()
+                ev1.synchronize()
+                ms += ev0.elapsed_time(ev1)
+            if keep is not None and keep.get("last"):
+                keep[j] = sim.tallies()
         return ms
 
     for i in range(args.warmup):
@@ -298,13 +354,12 @@ def ours_arm(args, w):
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
     dev_ms = 0.0
-    counters = None
+    last = {}
     for i in range(args.steps):
         flush.fill_(float(i))           # rewrite a 2x-L2 buffer between timed steps
         torch.cuda.synchronize()
-        dev_ms += step(args.warmup + i)
-        if i == args.steps - 1:
-            counters = sim.tallies()["counters"]
+        last["last"] = i == args.steps - 1
+        dev_ms += step(args.warmup + i, keep=last)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -316,24 +371,32 @@ def ours_arm(args, w):
         t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
-    total_photons = n * world * args.steps
+    total_photons = n * ncase * world * args.steps
     value = total_photons / (t_max * 1e-3)
 
-    # e2e through the public API with host buffers (fresh context state every step)
+    # e2e through the public API with host buffers: every step creates a context, sets
+    # the mesh (BVH + safety grid build, upload) and the other inputs from host arrays,
+    # then for each case sets its media, runs and copies all tallies back.
     e2e_v = h2d = d2h = None
+    e2e_steps = max(1, min(args.steps, 3))
     if rank == 0 or world > 1:
         e2e_t = 0.0
-        for i in range(max(1, min(args.steps, 3))):
+        for i in range(e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
+            h2d = d2h = 0
             with Simulation(local) as s2:
-                w.apply(s2, seed=0x4C50 + i)
-                s2.run(n, rank * n)
-                s2.tallies()
-                st2 = s2.stats()
+                w.apply(s2, seed=0x4C50 + 1 + i)
+                for j, c in enumerate(cases):
+                    if ncase > 1:
+                        s2.set_media(c.nmuasg)
+                    s2.zero()
+                    s2.run(n, (rank * ncase + j) * n)
+                    h2d += s2.stats()["h2d_bytes"]
+                    s2.tallies()
+                    d2h += s2.stats()["d2h_bytes"]
             e2e_t += time.perf_counter() - t0
-            h2d, d2h = st2["h2d_bytes"], st2["d2h_bytes"]
-        e2e_v = n * world * max(1, min(args.steps, 3)) / e2e_t
+        e2e_v = n * ncase * world * e2e_steps / e2e_t
 
     if dist is not None:
         red.clear()
@@ -345,42 +408,60 @@ def ours_arm(args, w):
 
     # roofline of the transport kernel (counters are global after the all-reduce)
     per_launch_photons = n * world
-    F, es, eb, eq = fp32_flops_per_photon(counters, per_launch_photons)
-    avg_kernel_ms = st["last_kernel_ms"]
-    achieved = F * n / (avg_kernel_ms * 1e-3) / 1e12
-    tpp = traffic_per_photon(w.name)
+    flops, launch_ms, events = 0.0, 0.0, {}
+    rse = {}
+    for j, c in enumerate(cases):
+        cnt = last[j]["counters"]
+        F, es, eb, eq = fp32_flops_per_photon(cnt, per_launch_photons)
+        ms_j = [k for jj, k in kernel_ms if jj == j]
+        flops += F * n * len(ms_j)
+        launch_ms += sum(ms_j)
+        events[c.name] = {"flops_per_photon": F, "scatter": es, "boundary": eb, "query": eq,
+                          "query_executed": cnt["query"] / per_launch_photons,
+                          "query_skipped_by_safety_grid": cnt["safe_skip"] / per_launch_photons,
+                          "avg_launch_ms": sum(ms_j) / len(ms_j)}
+        det = last[j]["det"]
+        if det.shape[0]:
+            r = ring_rse(det, per_launch_photons)
+            rse[c.name] = {"ring_rse": [float(x) for x in r],
+                           "photons_for_1pct_rse_at_farthest_ring": float(per_launch_photons * (r[-1] / 0.01) ** 2)}
+    achieved = flops / (launch_ms * 1e-3) / 1e12
+    traffic, traffic_photons = traffic_of(args.workload)
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None,
-            "traffic": (tpp * n) if tpp is not None else None,
+            "traffic": traffic,
+            "traffic_note": (f"DRAM bytes of one {traffic_photons}-photon launch (ncu, profiles/); the traffic is "
+                             f"the touch of the L2-resident tallies, safety grid and BVH and does not grow "
+                             f"with the photon count") if traffic is not None else None,
             "peak_source": "FP32 FMA peak measured in-run by lp_fp32_peak (MEASURED_PEAKS.json has no FP32 figure)",
-            "flops_per_photon": F,
-            "events_per_photon": {"scatter": es, "boundary": eb, "query": eq,
-                                  "query_executed": counters["query"] / per_launch_photons,
-                                  "query_skipped_by_safety_grid": counters["safe_skip"] / per_launch_photons}}
+            "events_per_photon": events}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            dt, n0 = run_reference_sample(w, threads, threads)
-            m = int(max(threads, min(w.n_photons, 12.0 / max(dt / n0, 1e-9))))
-            dt, k = run_reference_sample(w, m, threads)
+            m = reference_sample_size(cases, threads, 12.0)
+            dt, k = reference_sample(cases, m, threads)
             cpu = {"value": k / dt, "unit": "photons/s", "cores": threads, "kind": "reference",
-                   "sample": f"{k} photons of {w.name}: reference kernel source compiled for the CPU "
-                             f"(oracle/_ref) on {threads} threads + host binning"}
+                   "sample": f"{m} photons of each case of {workload_label(args, cases)}: the reference kernel "
+                             f"source compiled for the CPU (oracle/_ref, pencil beam source, brute-force triangle "
+                             f"search) on {threads} threads + ExecKernel's host binning"}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "photons/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
     line = {"metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name, "photons_per_step_per_gpu": n, "triangles": int(w.n_tri),
+            "config": {"workload": workload_label(args, cases), "photons_per_step_per_gpu": n * ncase,
+                       "photons_per_launch": n, "triangles": int(w.n_tri),
                        "parallelism": f"photon ranges x{world}" + (" + NCCL all-reduce of tallies" if world > 1 else ""),
                        "l2": "2x L2 buffer rewritten between timed steps",
+                       "arithmetic": "fast (FMA contraction, MCML direction cosines)",
                        "grid": st["grid"], "block": st["block"], "bvh_nodes": st["n_nodes"],
                        "bvh_nodes_in_smem": st["nodes_smem"], "tris_in_smem": st["tris_smem"]},
-            "wall_s": wall, "clocks": clk, "gpu_launches": args.steps,
+            "wall_s": wall, "clocks": clk, "gpu_launches": args.steps * ncase,
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "detector_error": rse,
             "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line))
     sim.close()
@@ -393,14 +474,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain_slab")
-    ap.add_argument("--photons", type=int, default=0, help="photons per step per GPU (default: workload's)")
+    ap.add_argument("--workload", default="curved_abdomen",
+                    help="curved_abdomen (660 + 940 nm per step), plain_slab, or another named workload")
+    ap.add_argument("--photons", type=int, default=0,
+                    help="photons per launch per GPU (default: the workload's, 1e7 for the abdomen)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    w = load_workload(args.workload, args.photons)
+    cases = load_cases(args.workload, args.photons)
     if args.impl == "reference":
-        return reference_arm(args, w)
-    return ours_arm(args, w)
+        return reference_arm(args, cases)
+    return ours_arm(args, cases)
 
 
 if __name__ == "__main__":
