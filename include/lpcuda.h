@@ -48,7 +48,8 @@ extern "C" {
 /* Counter slots of lp_tallies.counters */
 enum {
     LP_C_SCATTER = 0, LP_C_BOUNDARY, LP_C_QUERY, LP_C_ROULETTE, LP_C_MISS, LP_C_CAPPED,
-    LP_C_RZ_DROP, LP_C_VOX_DROP, LP_C_PHOTONS, LP_C_DRAWS, LP_C_SAFE_SKIP, LP_NCOUNTERS = 16
+    LP_C_RZ_DROP, LP_C_VOX_DROP, LP_C_PHOTONS, LP_C_DRAWS, LP_C_SAFE_SKIP, LP_C_BVH_QUERY,
+    LP_NCOUNTERS = 16
 };
 
 typedef struct lp_ctx lp_ctx;
@@ -127,12 +128,18 @@ int lp_set_extra_tallies(lp_ctx *ctx, const int32_t *vox_n, const float *vox_d,
  * operations (precomputed Henyey-Greenstein factors, direction-cosine scattering
  * update, vector refraction, reciprocal multiplies, FMA). */
 int lp_set_arithmetic(lp_ctx *ctx, int exact);
-/* Safety grid (no reference counterpart): a grid of at most max_cells cells over the
- * mesh bounds holding, per cell, a lower bound of the distance to the nearest
- * triangle, built on the device once per mesh (default 2^24 cells).  A step shorter
- * than the bound at the photon's position cannot reach a triangle, so its
- * nearest-triangle query is skipped without changing any result.  0 disables it. */
+/* Cell grid (no reference counterpart): a grid of at most max_cells cells over the
+ * mesh bounds, built on the device once per mesh (default 2^24 cells).  A cell that
+ * no triangle touches holds a lower bound of the distance to the nearest triangle: a
+ * step shorter than the bound at the photon's position cannot reach a triangle, so
+ * its nearest-triangle query is skipped.  A cell that triangles touch lists them: a
+ * short step's query tests only the triangles of the cells around the step instead of
+ * descending the BVH.  Neither changes any result.  0 disables the grid. */
 int lp_set_safety_grid(lp_ctx *ctx, int64_t max_cells);
+/* Whether cells touched by triangles list them (1, default) or hold no information
+ * (0: every query that the safety bound does not skip descends the BVH).  Results are
+ * identical either way; lp_query_triangles follows the same setting. */
+int lp_set_cell_lists(lp_ctx *ctx, int enable);
 /* Per-photon step cap (watchdog); photons that reach it are stopped and counted. */
 int lp_set_max_steps(lp_ctx *ctx, int64_t max_steps);
 /* Keep the per-photon float8 exit records of the next runs (RecordFSTxy,

@@ -17,7 +17,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "ou
 COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL, COMPAT_ALL = 1, 2, 4, 7
 NCOUNTERS = 16
 COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped", "rz_drop",
-                 "vox_drop", "photons", "draws", "safe_skip"]
+                 "vox_drop", "photons", "draws", "safe_skip", "bvh_query"]
 FIX_ONE = float(2 ** 32)
 
 _fp = C.POINTER(C.c_float)
@@ -92,6 +92,7 @@ _SIGS = {
     "lp_set_max_steps": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_set_arithmetic": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_safety_grid": ([C.c_void_p, C.c_int64], C.c_int),
+    "lp_set_cell_lists": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "lp_run_async": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),

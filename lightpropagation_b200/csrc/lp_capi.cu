@@ -7,6 +7,7 @@
 // CalculatePropagation.cpp:1446-1451) and accumulates fixed-point tallies on the
 // device.  No exceptions cross the ABI; errors are int codes plus a message.
 #include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -33,6 +34,10 @@ cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, u
                           cudaStream_t s);
 cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, uint16_t *out,
                                cudaStream_t s);
+cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, uint32_t *count, const uint32_t *start,
+                              int32_t *refs, cudaStream_t s);
+cudaError_t launch_cell_words(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start, bool lists,
+                              uint32_t *word, cudaStream_t s);
 double fma_peak_tflops(int num_sms);
 int block_size();
 }  // namespace lp
@@ -64,6 +69,10 @@ struct DevBuf {
         p = nullptr;
         n = 0;
     }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
 };
 
 }  // namespace
@@ -108,8 +117,11 @@ struct lp_ctx {
     // safety grid (lp_set_safety_grid)
     int64_t grid_max_cells = int64_t(1) << 24;
     bool grid_dirty = true;
-    DevBuf<uint16_t> safe;
-    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0;
+    bool cell_lists = true;
+    DevBuf<uint32_t> cell_word;
+    DevBuf<int32_t> cell_refs;
+    int64_t n_cell_refs = 0;
+    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0;
     int32_t g_n[3] = {0, 0, 0};
     float grid_ms = 0;
     // host copies of tallies
@@ -381,7 +393,10 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.exit_rec = c->exit_cap > 0 ? c->exit_rec.p : nullptr;
     P.exit_cap = c->exit_cap;
     P.work = c->work.p;
-    P.safe_grid = (c->grid_max_cells > 0 && c->safe.p && !c->grid_dirty) ? c->safe.p : nullptr;
+    const bool grid = c->grid_max_cells > 0 && c->cell_word.p && !c->grid_dirty;
+    P.cell_word = grid ? c->cell_word.p : nullptr;
+    P.cell_refs = (grid && c->cell_lists && c->n_cell_refs > 0) ? c->cell_refs.p : nullptr;
+    P.g_eps = c->g_eps;
     P.g_ox = c->g_origin[0];
     P.g_oy = c->g_origin[1];
     P.g_oz = c->g_origin[2];
@@ -392,13 +407,20 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.g_nz = c->g_n[2];
 }
 
-// Safety grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
-// the grid has at most grid_max_cells cells; values in units of h / 256.
+// Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
+// the grid has at most grid_max_cells cells; safety bounds in units of h / 256.
+//   1. safety_grid_kernel: per cell, a lower bound of the distance to the nearest triangle;
+//   2. cell_lists_kernel (count pass): per cell, the triangles touching it;
+//   3. exclusive scan of the counts: each cell's first slot in cell_refs;
+//   4. cell_lists_kernel (fill pass): the triangle indices;
+//   5. cell_word_kernel: one word per cell (KParams::cell_word).
 int build_safety_grid(lp_ctx *c)
 {
     c->grid_dirty = false;
+    c->n_cell_refs = 0;
     if (c->grid_max_cells <= 0 || c->n_tri == 0) {
-        c->safe.release();
+        c->cell_word.release();
+        c->cell_refs.release();
         return LP_OK;
     }
     const lp::Bvh &b = c->bvh;
@@ -423,8 +445,15 @@ int build_safety_grid(lp_ctx *c)
     if (cells > c->grid_max_cells) return fail(c, LP_ERR_RANGE, "safety grid: cannot fit %lld cells", (long long)cells);
     c->g_h = (float)h;
     c->g_unit = (float)(h / 256.0);
+    // list margin: far above the rounding of coordinates and of the ray/triangle test's
+    // intersection point at this scale, far below any cell size
+    c->g_eps = (float)(2e-5 * scale);
     for (int a = 0; a < 3; ++a) c->g_origin[a] = (float)(b.lo[a] - h);
-    LP_CUDA(c, c->safe.ensure((size_t)cells));
+    DevBuf<uint16_t> safe;
+    DevBuf<uint32_t> count, start;
+    DevBuf<unsigned char> scan_tmp;
+    LP_CUDA(c, safe.ensure((size_t)cells));
+    LP_CUDA(c, c->cell_word.ensure((size_t)cells));
     KParams P;
     std::memset(&P, 0, sizeof P);
     P.node_a = c->node_a.p; P.node_b = c->node_b.p; P.node_c = c->node_c.p; P.node_d = c->node_d.p;
@@ -432,20 +461,54 @@ int build_safety_grid(lp_ctx *c)
     P.g_ox = c->g_origin[0]; P.g_oy = c->g_origin[1]; P.g_oz = c->g_origin[2];
     P.g_nx = c->g_n[0]; P.g_ny = c->g_n[1]; P.g_nz = c->g_n[2];
     P.g_unit = c->g_unit;
+    P.g_inv_h = 1.0f / c->g_h;
     // eps: far above the few-ulp overreach of the ray/triangle test at this scale
     const float eps = (float)(1e-4 * scale);
+    cudaStream_t s = c->stream;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, c->stream);
+    cudaEventRecord(e0, s);
     cudaError_t e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h),
-                                           c->safe.p, c->stream);
-    cudaEventRecord(e1, c->stream);
+                                           safe.p, s);
+    bool lists = false;
+    if (e == cudaSuccess && c->cell_lists) {
+        const int nt = (int)c->bvh.tri_a.size();
+        size_t tmp_bytes = 0;
+        if ((e = count.ensure((size_t)cells)) == cudaSuccess && (e = start.ensure((size_t)cells)) == cudaSuccess &&
+            (e = cudaMemsetAsync(count.p, 0, (size_t)cells * 4, s)) == cudaSuccess &&
+            (e = lp::launch_cell_lists(P, nt, c->g_h, c->g_eps, count.p, nullptr, nullptr, s)) == cudaSuccess &&
+            (e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, count.p, start.p, cells, s)) == cudaSuccess &&
+            (e = scan_tmp.ensure(tmp_bytes)) == cudaSuccess &&
+            (e = cub::DeviceScan::ExclusiveSum(scan_tmp.p, tmp_bytes, count.p, start.p, cells, s)) == cudaSuccess) {
+            uint32_t last[2] = {0, 0};
+            if ((e = cudaMemcpyAsync(&last[0], start.p + cells - 1, 4, cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
+                (e = cudaMemcpyAsync(&last[1], count.p + cells - 1, 4, cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
+                (e = cudaStreamSynchronize(s)) == cudaSuccess) {
+                const int64_t total = (int64_t)last[0] + last[1];
+                // cells past 2^24 list entries are marked dense (BVH); beyond 2^28 lists are off
+                if (total > 0 && total <= (int64_t(1) << 28)) {
+                    if ((e = c->cell_refs.ensure((size_t)total)) == cudaSuccess &&
+                        (e = cudaMemsetAsync(count.p, 0, (size_t)cells * 4, s)) == cudaSuccess &&
+                        (e = lp::launch_cell_lists(P, nt, c->g_h, c->g_eps, count.p, start.p, c->cell_refs.p, s)) ==
+                            cudaSuccess) {
+                        lists = true;
+                        c->n_cell_refs = total;
+                    }
+                }
+            }
+        }
+    }
+    if (e == cudaSuccess)
+        e = lp::launch_cell_words(cells, safe.p, lists ? count.p : nullptr, lists ? start.p : nullptr, lists,
+                                  c->cell_word.p, s);
+    cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     cudaEventElapsedTime(&c->grid_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (e != cudaSuccess) return cuda_fail(c, e, "safety grid");
+    if (e != cudaSuccess) return cuda_fail(c, e, "cell grid");
+    if (!lists) c->cell_refs.release();
     return LP_OK;
 }
 
@@ -511,7 +574,8 @@ void lp_destroy(lp_ctx *c)
     c->sft.release(); c->rtd.release(); c->rz.release(); c->vox.release(); c->rbins.release();
     c->region.release(); c->det.release(); c->counters.release(); c->work.release();
     c->exit_rec.release();
-    c->safe.release();
+    c->cell_word.release();
+    c->cell_refs.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -655,6 +719,16 @@ int lp_set_safety_grid(lp_ctx *c, int64_t max_cells)
     if (max_cells < 0 || max_cells > (int64_t(1) << 28)) return fail(c, LP_ERR_RANGE, "lp_set_safety_grid: %lld cells", (long long)max_cells);
     c->grid_max_cells = max_cells;
     c->grid_dirty = true;
+    return LP_OK;
+}
+
+int lp_set_cell_lists(lp_ctx *c, int enable)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_cell_lists: ctx is NULL");
+    if ((enable != 0) != c->cell_lists) {
+        c->cell_lists = enable != 0;
+        c->grid_dirty = true;
+    }
     return LP_OK;
 }
 
@@ -867,6 +941,7 @@ int lp_query_triangles(lp_ctx *c, int64_t n, const float *orig, const float *dir
     LP_CUDA(c, cudaSetDevice(c->device));
     int ur = upload_mesh(c);
     if (ur) return ur;
+    if (c->grid_dirty && (ur = build_safety_grid(c))) return ur;
     DevBuf<float> o, d, tm, to;
     DevBuf<int32_t> rf, io;
     LP_CUDA(c, o.ensure((size_t)n * 3));

@@ -66,25 +66,40 @@ struct KParams {
     float det_lo[kMaxDet], det_hi[kMaxDet];
     float *exit_rec;
     int64_t exit_cap;
-    // safety grid: per cell a lower bound of the distance from any point of the cell to
-    // the nearest triangle, in units of g_unit (0 = unknown / near a surface)
-    const uint16_t *safe_grid;
-    float g_ox, g_oy, g_oz, g_inv_h, g_unit;
+    // cell grid over the mesh bounds (cubic cells of size 1 / g_inv_h), one word per cell:
+    //   kCellEmpty set:   no triangle touches the cell; bits 0-15 hold a lower bound of
+    //                     the distance from any point of the cell to the nearest
+    //                     triangle, in units of g_unit
+    //   kCellEmpty clear: bits 0-23 = first entry in cell_refs, bits 24-30 = number of
+    //                     triangles touching the cell (kCellDense: too many, use the BVH)
+    // cell_refs holds BVH-order triangle indices.  Null cell_word: BVH queries only.
+    const uint32_t *cell_word;
+    const int32_t *cell_refs;   // null: the words carry safety bounds only
+    float g_ox, g_oy, g_oz, g_inv_h, g_unit, g_eps;
     int32_t g_nx, g_ny, g_nz;
     // scratch: photon work counter
     unsigned long long *work;
 };
 
-// Conservative distance from p to the nearest triangle, read from the safety grid.
-__device__ __forceinline__ float safe_distance(const KParams &P, float px, float py, float pz)
+constexpr uint32_t kCellEmpty = 0x80000000u;
+constexpr uint32_t kCellDense = 127u;
+constexpr int kLocalMaxCells = 8;   // larger segment boxes go to the BVH
+
+// The cell word at p; points outside the grid read as an empty cell with bound 0.
+__device__ __forceinline__ uint32_t cell_at(const KParams &P, float px, float py, float pz)
 {
-    if (!P.safe_grid) return 0.0f;
+    if (!P.cell_word) return kCellEmpty;
     const int ix = (int)floorf((px - P.g_ox) * P.g_inv_h);
     const int iy = (int)floorf((py - P.g_oy) * P.g_inv_h);
     const int iz = (int)floorf((pz - P.g_oz) * P.g_inv_h);
-    if (ix < 0 || iy < 0 || iz < 0 || ix >= P.g_nx || iy >= P.g_ny || iz >= P.g_nz) return 0.0f;
-    const unsigned short q = __ldg(P.safe_grid + ((int64_t)iz * P.g_ny + iy) * P.g_nx + ix);
-    return (float)q * P.g_unit;
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= P.g_nx || iy >= P.g_ny || iz >= P.g_nz) return kCellEmpty;
+    return __ldg(P.cell_word + ((int64_t)iz * P.g_ny + iy) * P.g_nx + ix);
+}
+
+// Conservative distance from p to the nearest triangle (0 near a surface).
+__device__ __forceinline__ float safe_distance(const KParams &P, uint32_t word)
+{
+    return (word & kCellEmpty) ? (float)(word & 0xffffu) * P.g_unit : 0.0f;
 }
 
 // ----------------------------------------------------------------- Philox4x32-10
@@ -276,6 +291,49 @@ __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int 
             node = stack[--sp];
         }
     }
+    if (bid == 0x7fffffff) {
+        t_out = kNoHit;
+        return -1;
+    }
+    t_out = best;
+    return bid;
+}
+
+// The same query answered from the cell grid when the segment [p, p + bound v] is short:
+// every triangle that touches a cell overlapping the segment's bounding box (widened by
+// g_eps) is tested with test_tri, so the candidate set holds every triangle the test can
+// accept within the bound, and the result (nearest t, then lowest original index) is
+// the BVH's bit for bit.  Boxes of more than kLocalMaxCells cells, or a dense cell, go
+// to query_nearest; *used_bvh reports which path answered.
+__device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri,
+                                          float bound, float &t_out, bool &used_bvh)
+{
+    used_bvh = true;
+    if (!P.cell_refs || !(bound < kNoHit)) return query_nearest(M, p, v, ref_tri, bound, t_out);
+    const float e = P.g_eps;
+    const float qx = p.x + bound * v.x, qy = p.y + bound * v.y, qz = p.z + bound * v.z;
+    const int nx = P.g_nx, ny = P.g_ny, nz = P.g_nz;
+    const int x0 = min(max((int)floorf((fminf(p.x, qx) - e - P.g_ox) * P.g_inv_h), 0), nx - 1);
+    const int x1 = min(max((int)floorf((fmaxf(p.x, qx) + e - P.g_ox) * P.g_inv_h), 0), nx - 1);
+    const int y0 = min(max((int)floorf((fminf(p.y, qy) - e - P.g_oy) * P.g_inv_h), 0), ny - 1);
+    const int y1 = min(max((int)floorf((fmaxf(p.y, qy) + e - P.g_oy) * P.g_inv_h), 0), ny - 1);
+    const int z0 = min(max((int)floorf((fminf(p.z, qz) - e - P.g_oz) * P.g_inv_h), 0), nz - 1);
+    const int z1 = min(max((int)floorf((fmaxf(p.z, qz) + e - P.g_oz) * P.g_inv_h), 0), nz - 1);
+    if ((x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1) > kLocalMaxCells)
+        return query_nearest(M, p, v, ref_tri, bound, t_out);
+    float best = bound;
+    int bid = 0x7fffffff;
+    for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y)
+            for (int x = x0; x <= x1; ++x) {
+                const uint32_t w = __ldg(P.cell_word + ((int64_t)z * ny + y) * nx + x);
+                if (w & kCellEmpty) continue;
+                const uint32_t cnt = (w >> 24) & 127u;
+                if (cnt == kCellDense) return query_nearest(M, p, v, ref_tri, bound, t_out);
+                const int32_t *r = P.cell_refs + (w & 0xffffffu);
+                for (uint32_t k = 0; k < cnt; ++k) test_tri(M, __ldg(r + k), p, v, ref_tri, best, bid);
+            }
+    used_bvh = false;
     if (bid == 0x7fffffff) {
         t_out = kNoHit;
         return -1;

@@ -132,4 +132,101 @@ cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float
     return cudaGetLastError();
 }
 
+// Triangle / cube overlap by the separating-axis theorem: the cube c +- r and the
+// triangle (a, b, d) are disjoint iff their projections are disjoint on one of 13
+// axes: the 3 cube axes, the triangle normal, and the 9 cross products of a cube axis
+// with a triangle edge (Akenine-Moller, "Fast 3D triangle-box overlap testing", 2001).
+// r includes a margin far above the rounding of the projections, so the test never
+// reports "disjoint" for a triangle that touches the cube.
+__device__ bool tri_cube_overlap(V3 c, float r, V3 a, V3 b, V3 d)
+{
+    const V3 v0 = sub3(a, c), v1 = sub3(b, c), v2 = sub3(d, c);
+    if (fminf(v0.x, fminf(v1.x, v2.x)) > r || fmaxf(v0.x, fmaxf(v1.x, v2.x)) < -r) return false;
+    if (fminf(v0.y, fminf(v1.y, v2.y)) > r || fmaxf(v0.y, fmaxf(v1.y, v2.y)) < -r) return false;
+    if (fminf(v0.z, fminf(v1.z, v2.z)) > r || fmaxf(v0.z, fmaxf(v1.z, v2.z)) < -r) return false;
+    const V3 e[3] = {sub3(v1, v0), sub3(v2, v1), sub3(v0, v2)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const V3 f = e[i];
+        // axis x cross f = (0, -f.z, f.y)
+        float p0 = f.y * v0.z - f.z * v0.y, p1 = f.y * v1.z - f.z * v1.y, p2 = f.y * v2.z - f.z * v2.y;
+        float rr = r * (fabsf(f.y) + fabsf(f.z));
+        if (fminf(p0, fminf(p1, p2)) > rr || fmaxf(p0, fmaxf(p1, p2)) < -rr) return false;
+        // axis y cross f = (f.z, 0, -f.x)
+        p0 = f.z * v0.x - f.x * v0.z; p1 = f.z * v1.x - f.x * v1.z; p2 = f.z * v2.x - f.x * v2.z;
+        rr = r * (fabsf(f.x) + fabsf(f.z));
+        if (fminf(p0, fminf(p1, p2)) > rr || fmaxf(p0, fmaxf(p1, p2)) < -rr) return false;
+        // axis z cross f = (-f.y, f.x, 0)
+        p0 = f.x * v0.y - f.y * v0.x; p1 = f.x * v1.y - f.y * v1.x; p2 = f.x * v2.y - f.y * v2.x;
+        rr = r * (fabsf(f.x) + fabsf(f.y));
+        if (fminf(p0, fminf(p1, p2)) > rr || fmaxf(p0, fmaxf(p1, p2)) < -rr) return false;
+    }
+    const V3 n = cross3(e[0], e[1]);
+    return fabsf(dot3(n, v0)) <= r * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
+}
+
+// One pass over the triangles (BVH order): every cell that a triangle touches (cells
+// widened by eps) gets a count (refs == nullptr) or, in the second pass, the triangle's
+// index at start[cell] + the next free slot (count re-zeroed before that pass).
+__global__ void __launch_bounds__(256) cell_lists_kernel(const __grid_constant__ KParams P, int n_tri, float h,
+                                                         float eps, uint32_t *count, const uint32_t *start,
+                                                         int32_t *refs)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_tri; j += gridDim.x * blockDim.x) {
+        const float4 ta = __ldg(P.tri_a + j), tb = __ldg(P.tri_b + j), tc = __ldg(P.tri_c + j);
+        const V3 a = v3(ta.x, ta.y, ta.z);
+        const V3 b = add3(a, v3(ta.w, tb.x, tb.y)), d = add3(a, v3(tb.z, tb.w, tc.x));
+        const float lo[3] = {fminf(a.x, fminf(b.x, d.x)), fminf(a.y, fminf(b.y, d.y)), fminf(a.z, fminf(b.z, d.z))};
+        const float hi[3] = {fmaxf(a.x, fmaxf(b.x, d.x)), fmaxf(a.y, fmaxf(b.y, d.y)), fmaxf(a.z, fmaxf(b.z, d.z))};
+        const float o[3] = {P.g_ox, P.g_oy, P.g_oz};
+        const int n[3] = {P.g_nx, P.g_ny, P.g_nz};
+        int c0[3], c1[3];
+        for (int k = 0; k < 3; ++k) {
+            c0[k] = min(max((int)floorf((lo[k] - eps - o[k]) * P.g_inv_h), 0), n[k] - 1);
+            c1[k] = min(max((int)floorf((hi[k] + eps - o[k]) * P.g_inv_h), 0), n[k] - 1);
+        }
+        for (int z = c0[2]; z <= c1[2]; ++z)
+            for (int y = c0[1]; y <= c1[1]; ++y)
+                for (int x = c0[0]; x <= c1[0]; ++x) {
+                    const V3 c = v3(o[0] + ((float)x + 0.5f) * h, o[1] + ((float)y + 0.5f) * h,
+                                    o[2] + ((float)z + 0.5f) * h);
+                    if (!tri_cube_overlap(c, 0.5f * h + eps, a, b, d)) continue;
+                    const int64_t cell = ((int64_t)z * n[1] + y) * n[0] + x;
+                    const uint32_t k = atomicAdd(count + cell, 1u);
+                    if (refs) refs[start[cell] + k] = j;
+                }
+    }
+}
+
+// Cell words from the safety bounds and the list layout (see KParams::cell_word).
+// lists == false: every cell carries its safety bound only.
+__global__ void cell_word_kernel(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start,
+                                 bool lists, uint32_t *word)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = lists ? count[i] : 0u;
+        uint32_t w;
+        if (k == 0) w = kCellEmpty | safe[i];
+        else if (k >= kCellDense || start[i] + k > 0xffffffu) w = kCellDense << 24;
+        else w = start[i] | (k << 24);
+        word[i] = w;
+    }
+}
+
+cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, uint32_t *count, const uint32_t *start,
+                              int32_t *refs, cudaStream_t s)
+{
+    const int grid = std::max(1, std::min((n_tri + 255) / 256, 148 * 16));
+    cell_lists_kernel<<<grid, 256, 0, s>>>(P, n_tri, h, eps, count, start, refs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_words(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start, bool lists,
+                              uint32_t *word, cudaStream_t s)
+{
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    cell_word_kernel<<<grid, 256, 0, s>>>(n, safe, count, start, lists, word);
+    return cudaGetLastError();
+}
+
 }  // namespace lp

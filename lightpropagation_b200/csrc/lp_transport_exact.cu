@@ -29,7 +29,8 @@ __global__ void __launch_bounds__(kBlock) query_kernel(const __grid_constant__ K
         const V3 p = v3(orig[3 * i], orig[3 * i + 1], orig[3 * i + 2]);
         const V3 v = v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
         float t;
-        id_out[i] = query_nearest(M, p, v, ref[i], tmax[i], t);
+        bool used_bvh;
+        id_out[i] = cell_query(P, M, p, v, ref[i], tmax[i], t, used_bvh);
         t_out[i] = t;
     }
 }

@@ -49,7 +49,7 @@ enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2 };
 enum : uint32_t { EXIT_NONE = 0, EXIT_SURF = 1, EXIT_SURF_FETAL = 2, EXIT_TRANS = 3 };
 
 struct Counters {
-    uint32_t scatter, boundary, query, roulette, rz_drop, vox_drop, skip;
+    uint32_t scatter, boundary, query, roulette, rz_drop, vox_drop, skip, bvh;
 };
 
 template <bool Exact>
@@ -285,14 +285,20 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     float thit;
     int tri;
     const V3 p = v3(ph.px, ph.py, ph.pz), v = v3(ph.vx, ph.vy, ph.vz);
-    if (!m.ambient && step < safe_distance(P, p.x, p.y, p.z)) {
+    if (m.ambient) {
+        tri = query_nearest(M, p, v, ph.refTri, kNoHit, thit);
+        cnt.query++;
+        cnt.bvh++;
+    } else if (step < safe_distance(P, cell_at(P, p.x, p.y, p.z))) {
         // no triangle within the step: the bounded query would return "no hit"
         tri = -1;
         thit = kNoHit;
         cnt.skip++;
     } else {
-        tri = query_nearest(M, p, v, ph.refTri, m.ambient ? kNoHit : step, thit);
+        bool used_bvh;
+        tri = cell_query(P, M, p, v, ph.refTri, step, thit, used_bvh);
         cnt.query++;
+        cnt.bvh += used_bvh ? 1u : 0u;
     }
     if (m.ambient) step = thit;
     const bool boundary = (tri >= 0) ? (thit <= step) : (kNoHit <= step);
@@ -575,6 +581,9 @@ __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_const
         x = cnt.skip;
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0 && x) atomicAdd(s_cnt + 10, x);
+        x = cnt.bvh;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0 && x) atomicAdd(s_cnt + 11, x);
     }
     __syncthreads();
     if (threadIdx.x < 16 && s_cnt[threadIdx.x]) atomicAdd(P.counters + threadIdx.x, s_cnt[threadIdx.x]);

@@ -112,6 +112,11 @@ class Simulation:
         """Cells of the query-skipping safety grid (0 disables it; results are unchanged)."""
         self._ck(self._L.lp_set_safety_grid(self._h, int(max_cells)))
 
+    def set_cell_lists(self, enable: bool):
+        """Cells touched by triangles list them for short-step queries (default on;
+        results are unchanged either way)."""
+        self._ck(self._L.lp_set_cell_lists(self._h, 1 if enable else 0))
+
     def set_max_steps(self, n: int):
         self._ck(self._L.lp_set_max_steps(self._h, int(n)))
 

@@ -74,8 +74,11 @@ def _soup(rng, n):
     return t.reshape(n, 9)
 
 
-@pytest.mark.parametrize("mesh", ["slab", "soup", "abdomen"])
-def test_bvh_query_matches_brute_force(oracle_lib, mesh):
+@pytest.mark.parametrize("mesh,lists", [("slab", False), ("slab", True), ("soup", False), ("soup", True),
+                                        ("abdomen", False), ("abdomen", True)])
+def test_bvh_query_matches_brute_force(oracle_lib, mesh, lists):
+    """Nearest-triangle queries, answered by the BVH (lists off) or by the cell lists for
+    short segments (lists on), equal the reference's full scan bit for bit."""
     rng = np.random.default_rng(11)
     if mesh == "slab":
         tri, nrm, med = meshes.layered_slab([2.0, 10.0, 30.0])
@@ -102,9 +105,12 @@ def test_bvh_query_matches_brute_force(oracle_lib, mesh):
     d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
     ref = np.full(n, -1, np.int32)
     ref[:k] = pick
-    tmax = np.where(rng.random(n) < 0.5, 10000.0, rng.exponential(5.0, n)).astype(np.float32)
+    u = rng.random(n)
+    tmax = np.where(u < 0.3, 10000.0, np.where(u < 0.6, rng.exponential(5.0, n),
+                                               rng.exponential(0.2, n))).astype(np.float32)
     with Simulation(0) as s:
         s.set_mesh(tri, nrm, med)
+        s.set_cell_lists(lists)
         ids, ts = s.query(orig, d, ref, tmax)
     L = po.lib()
     trif = np.ascontiguousarray(tri, np.float32).ravel()
@@ -182,26 +188,33 @@ def test_fast_matches_reference_arithmetic_high_statistics(slab):
 
 @pytest.mark.parametrize("case,exact", [("slab", False), ("abdomen", False), ("abdomen", True)])
 def test_safety_grid_changes_nothing(slab, case, exact):
-    """Skipping queries whose step cannot reach a triangle must leave every tally
-    bit-identical; the grid must also actually skip queries."""
+    """Skipping queries whose step cannot reach a triangle, and answering short-step
+    queries from the cell lists, must leave every tally bit-identical to BVH-only
+    transport; the grid must also actually skip queries and the lists replace BVH
+    descents."""
     w = slab if case == "slab" else workloads.curved_abdomen(freq=20)
     n = 20000
     out = []
-    for cells in (0, 1 << 22):
+    for cells, lists in ((0, False), (1 << 22, False), (1 << 22, True)):
         with Simulation(0) as s:
             w.apply(s, seed=31)
             s.set_arithmetic(exact)
             s.set_safety_grid(cells)
+            s.set_cell_lists(lists)
             s.zero()
             s.run(n)
             out.append(s.tallies())
-    a, b = out
+    a, b, c = out
     for k in ("sft", "rtd", "rz", "vox", "rbins", "region", "det"):
         assert np.array_equal(a[k], b[k]), k
-    ca, cb = a["counters"], b["counters"]
-    assert ca["scatter"] == cb["scatter"] and ca["boundary"] == cb["boundary"]
+        assert np.array_equal(a[k], c[k]), k
+    ca, cb, cc = a["counters"], b["counters"], c["counters"]
+    assert ca["scatter"] == cb["scatter"] == cc["scatter"] and ca["boundary"] == cb["boundary"] == cc["boundary"]
     assert ca["safe_skip"] == 0 and cb["safe_skip"] > 0.3 * cb["scatter"]
     assert cb["query"] + cb["safe_skip"] == ca["query"]
+    assert cc["query"] + cc["safe_skip"] == ca["query"]
+    assert ca["bvh_query"] == ca["query"] and cb["bvh_query"] == cb["query"]
+    assert cc["bvh_query"] < 0.5 * cc["query"], (cc["bvh_query"], cc["query"])
 
 
 def test_determinism_and_split_runs(slab):
