@@ -374,6 +374,27 @@ def ours_arm(args, cases):
     total_photons = n * ncase * world * args.steps
     value = total_photons / (t_max * 1e-3)
 
+    # gradient cost: one differentiated launch per case (adjoint sums of d(ring signal) /
+    # d(mua, mus) for every region) against the mean plain launch of the timed steps
+    gradient = None
+    if rank == 0 and not args.no_gradient and sim._rings.shape[0] and cases[0].nmuasg.shape[0] <= 8:
+        grad_ms, plain_ms = 0.0, 0.0
+        for j, c in enumerate(cases):
+            if ncase > 1:
+                sim.set_media(c.nmuasg)
+            sim.set_gradient(True)
+            sim.zero()
+            flush.fill_(0.0)
+            sim.run(n, 10 ** 12 + j * n)
+            grad_ms += sim.kernel_ms()
+            sim.set_gradient(False)
+            ms_j = [k for jj, k in kernel_ms if jj == j]
+            plain_ms += sum(ms_j) / len(ms_j)
+        gradient = {"cost_vs_forward": grad_ms / plain_ms, "grad_launch_ms": grad_ms / ncase,
+                    "forward_launch_ms": plain_ms / ncase,
+                    "derivatives": int(sim._rings.shape[0] * (cases[0].nmuasg.shape[0] - 1) * 2 * ncase),
+                    "what": "one launch per case giving d(ring signal)/d(mua, mus) of every region and ring"}
+
     # e2e through the public API with host buffers: every step creates a context, sets
     # the mesh (BVH + safety grid build, upload) and the other inputs from host arrays,
     # then for each case sets its media, runs and copies all tallies back.
@@ -461,7 +482,7 @@ def ours_arm(args, cases):
                        "bvh_nodes_in_smem": st["nodes_smem"], "tris_in_smem": st["tris_smem"]},
             "wall_s": wall, "clocks": clk, "gpu_launches": args.steps * ncase,
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "detector_error": rse,
+            "detector_error": rse, "gradient": gradient,
             "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line))
     sim.close()
@@ -479,6 +500,7 @@ def main():
     ap.add_argument("--photons", type=int, default=0,
                     help="photons per launch per GPU (default: the workload's, 1e7 for the abdomen)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the gradient-cost launches")
     args = ap.parse_args()
     cases = load_cases(args.workload, args.photons)
     if args.impl == "reference":

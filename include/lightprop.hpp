@@ -157,6 +157,10 @@ public:
     void SetSeed(uint64_t s) { seed_ = s; }
     void SetCompat(uint32_t c) { compat_ = c; }
     void SetFiberSource(float radius, float na) { fiberR_ = radius; fiberNA_ = na; }
+    // ring detectors (no reference counterpart): [inner, outer) radii in the emitter
+    // plane, two floats per ring; surface exits inside a ring are scored there
+    void SetRingDetectors(const std::vector<float> &radii) { rings_ = radii; }
+    const std::vector<float> &GetTissueTable() const { return nmuasG_; }   // n, mua, mus, g per region
 
     int64_t GetNumberOfPhotons() const { return photons_; }
     float GetChanceForRoulette() const { return chance_; }
@@ -189,6 +193,7 @@ private:
     float eP0XYZ_[12] = {0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1};
     int fetalTissueID_ = 1, interactions_ = 100;
     float ppu_ = 100, chance_ = 0.5f, wth_ = 0.001f, fiberR_ = 0, fiberNA_ = 0;
+    std::vector<float> rings_;
     int64_t photons_ = 1;
     uint64_t seed_ = 0x4C50;
     uint32_t compat_ = 7;
@@ -197,6 +202,34 @@ private:
     std::vector<double> region_;
     std::string err_;
     int check(int rc);
+};
+
+// ------------------------------------------------------------------ differentiation
+// Ring-detector signals S_d as a function of every region's absorption and scattering
+// coefficients, shaped like an autograd Function: Forward traces photons with the
+// adjoint path-length / interaction sums on (lp_forward) and keeps the Jacobians,
+// Backward returns the vector-Jacobian product.  Mesh, source and rings come from an
+// initialised CalculatePropagation.  No reference counterpart.
+class TransportFunction {
+public:
+    explicit TransportFunction(CalculatePropagation &cp) : cp_(cp) {}
+    // S_d for photons [first, first + n) with mua[r], mus[r] replacing the regions'
+    // coefficients (n and g unchanged); empty on failure (see LastError)
+    std::vector<double> Forward(const std::vector<float> &mua, const std::vector<float> &mus, int64_t n,
+                                int64_t first = 0);
+    // grad_mua[r] = sum_d grad_signal[d] dS_d/dmua_r, grad_mus likewise; false on failure
+    bool Backward(const std::vector<double> &grad_signal, std::vector<double> &grad_mua,
+                  std::vector<double> &grad_mus) const;
+    const std::vector<double> &JacobianMua() const { return jmua_; }   // [n_det][n_media]
+    const std::vector<double> &JacobianMus() const { return jmus_; }
+    const std::vector<double> &SignalError() const { return signal_se_; }
+    const std::string &LastError() const { return err_; }
+
+private:
+    CalculatePropagation &cp_;
+    std::vector<double> jmua_, jmus_, signal_se_;
+    int n_det_ = 0, n_media_ = 0;
+    mutable std::string err_;
 };
 
 // ------------------------------------------------------------------ analysis

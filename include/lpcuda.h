@@ -136,6 +136,38 @@ int lp_set_arithmetic(lp_ctx *ctx, int exact);
  * short step's query tests only the triangles of the cells around the step instead of
  * descending the BVH.  Neither changes any result.  0 disables the grid. */
 int lp_set_safety_grid(lp_ctx *ctx, int64_t max_cells);
+/* ---- Differentiation (no reference counterpart) ---------------------------------
+ * Derivatives of the ring-detector signals S_d (mean surface weight per launched
+ * photon scored in ring d of lp_set_extra_tallies) with respect to the absorption and
+ * scattering coefficients of every region, accumulated in the same pass as the
+ * forward run.  Each photon keeps its path length L_r and interaction count k_r per
+ * region (FP32); a photon scored with weight s in ring d adds s * (-L_r / factor) to
+ * dS_d/dmua_r and s * (k_r / mus_r - L_r / factor) to dS_d/dmus_r (perturbation Monte
+ * Carlo).  The sums are FP64.  At most 8 regions. */
+int lp_set_gradient(lp_ctx *ctx, int enable);
+
+typedef struct lp_gradient {
+    int32_t n_det, n_media;
+    int64_t n_photons;        /* photons the sums cover (since the tallies were zeroed) */
+    const double *signal;     /* [n_det]           S_d                                   */
+    const double *signal_se;  /* [n_det]           standard error of S_d                  */
+    const double *d_mua;      /* [n_det][n_media]  dS_d / dmua_r                         */
+    const double *d_mus;      /* [n_det][n_media]  dS_d / dmus_r                         */
+    const double *d_mua_se;   /* [n_det][n_media]  standard errors of the derivatives     */
+    const double *d_mus_se;
+} lp_gradient;
+/* Reads the sums back and forms signals and derivatives.  The arrays are owned by
+ * ctx and stay valid until the next lp_get_gradient / lp_forward / lp_destroy. */
+int lp_get_gradient(lp_ctx *ctx, lp_gradient *out);
+/* Forward half of an autograd-style function: zero the tallies, trace photons
+ * [first, first + n) with differentiation on, and write S_d to signal[n_det]
+ * (may be NULL). */
+int lp_forward(lp_ctx *ctx, int64_t first, int64_t n, double *signal);
+/* Backward half, the vector-Jacobian product of the last lp_forward:
+ * grad_mua[r] = sum_d grad_signal[d] dS_d/dmua_r and grad_mus likewise, n_media
+ * entries each. */
+int lp_backward(lp_ctx *ctx, const double *grad_signal, double *grad_mua, double *grad_mus);
+
 /* Whether cells touched by triangles list them (1, default) or hold no information
  * (0: every query that the safety bound does not skip descends the BVH).  Results are
  * identical either way; lp_query_triangles follows the same setting. */

@@ -66,6 +66,15 @@ class NoAllocArgs(C.Structure):
 
 
 NOALLOC_MAX_TRI, NOALLOC_MAX_MEDIA = 4096, 64
+GRAD_MAX_REGIONS = 8
+
+_dp = C.POINTER(C.c_double)
+
+
+class Gradient(C.Structure):
+    """lp_gradient: ring signals and their derivatives (arrays owned by the context)."""
+    _fields_ = [("n_det", C.c_int32), ("n_media", C.c_int32), ("n_photons", C.c_int64)] + \
+        [(n, _dp) for n in ("signal", "signal_se", "d_mua", "d_mus", "d_mua_se", "d_mus_se")]
 
 
 class LPError(RuntimeError):
@@ -108,6 +117,10 @@ _SIGS = {
     "lp_get_device_tallies": ([C.c_void_p, C.POINTER(DeviceTallies)], C.c_int),
     "lp_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
     "lp_run_noalloc": ([C.POINTER(NoAllocArgs), C.c_void_p], C.c_int),
+    "lp_set_gradient": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_get_gradient": ([C.c_void_p, C.POINTER(Gradient)], C.c_int),
+    "lp_forward": ([C.c_void_p, C.c_int64, C.c_int64, _dp], C.c_int),
+    "lp_backward": ([C.c_void_p, _dp, _dp, _dp], C.c_int),
 }
 
 EXPORTED = sorted(_SIGS)

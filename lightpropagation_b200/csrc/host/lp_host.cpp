@@ -198,7 +198,59 @@ int CalculatePropagation::Init()
     if (check(lp_set_fiber_source(ctx_, fiberR_, fiberNA_))) return 1;
     if (check(lp_set_tally_grid(ctx_, dimensions_.data(), detGrid_.data(), fetalTissueID_))) return 1;
     if (check(lp_set_params(ctx_, chance_, wth_, ppu_, seed_, compat_))) return 1;
+    if (!rings_.empty()) {
+        const int32_t vox_n[3] = {0, 0, 0};
+        const float vox_d[3] = {1, 1, 1};
+        if (check(lp_set_extra_tallies(ctx_, vox_n, vox_d, 0, 1.0f, (int32_t)(rings_.size() / 2), rings_.data())))
+            return 1;
+    }
     return check(lp_zero_tallies(ctx_));
+}
+
+// ------------------------------------------------------------------ TransportFunction
+std::vector<double> TransportFunction::Forward(const std::vector<float> &mua, const std::vector<float> &mus,
+                                               int64_t n, int64_t first)
+{
+    lp_ctx *ctx = cp_.Context();
+    std::vector<float> table = cp_.GetTissueTable();
+    const size_t R = table.size() / 4;
+    if (!ctx || mua.size() != R || mus.size() != R) {
+        err_ = "TransportFunction::Forward: Init() first; mua and mus need one value per region";
+        return {};
+    }
+    for (size_t r = 0; r < R; ++r) {
+        table[4 * r + 1] = mua[r];
+        table[4 * r + 2] = mus[r];
+    }
+    lp_gradient g;
+    if (lp_set_media(ctx, (int32_t)R, table.data()) || lp_forward(ctx, first, n, nullptr) ||
+        lp_get_gradient(ctx, &g)) {
+        err_ = lp_last_error(ctx);
+        return {};
+    }
+    n_det_ = g.n_det;
+    n_media_ = g.n_media;
+    jmua_.assign(g.d_mua, g.d_mua + (size_t)n_det_ * n_media_);
+    jmus_.assign(g.d_mus, g.d_mus + (size_t)n_det_ * n_media_);
+    signal_se_.assign(g.signal_se, g.signal_se + n_det_);
+    return std::vector<double>(g.signal, g.signal + n_det_);
+}
+
+bool TransportFunction::Backward(const std::vector<double> &grad_signal, std::vector<double> &grad_mua,
+                                 std::vector<double> &grad_mus) const
+{
+    if ((int)grad_signal.size() != n_det_ || n_media_ == 0) {
+        err_ = "TransportFunction::Backward: one upstream gradient per ring after a Forward";
+        return false;
+    }
+    grad_mua.assign((size_t)n_media_, 0.0);
+    grad_mus.assign((size_t)n_media_, 0.0);
+    for (int d = 0; d < n_det_; ++d)
+        for (int r = 0; r < n_media_; ++r) {
+            grad_mua[r] += grad_signal[d] * jmua_[(size_t)d * n_media_ + r];
+            grad_mus[r] += grad_signal[d] * jmus_[(size_t)d * n_media_ + r];
+        }
+    return true;
 }
 
 int CalculatePropagation::Propagation()

@@ -27,6 +27,8 @@ cudaError_t launch_transport_fast(const KParams &P, int grid, int smem, cudaStre
 cudaError_t transport_occupancy_fast(int smem, int *blocks_per_sm);
 cudaError_t launch_transport_exact(const KParams &P, int grid, int smem, cudaStream_t s);
 cudaError_t transport_occupancy_exact(int smem, int *blocks_per_sm);
+cudaError_t transport_occupancy_fast_grad(int smem, int *blocks_per_sm);
+cudaError_t transport_occupancy_exact_grad(int smem, int *blocks_per_sm);
 cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *orig, const float *dir,
                          const int32_t *ref, const float *tmax, int32_t *id_out, float *t_out,
                          cudaStream_t s);
@@ -124,6 +126,10 @@ struct lp_ctx {
     float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0;
     int32_t g_n[3] = {0, 0, 0};
     float grid_ms = 0;
+    // differentiation (lp_set_gradient / lp_forward / lp_backward)
+    bool grad_on = false;
+    DevBuf<double> grad;                  // [kMaxDet][kGradRegions][5], see KParams::grad
+    std::vector<double> h_grad, g_signal, g_signal_se, g_mua, g_mus, g_mua_se, g_mus_se;
     // host copies of tallies
     std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
     float last_ms = 0.0f;
@@ -202,6 +208,7 @@ int alloc_tallies(lp_ctx *c)
     LP_CUDA(c, c->det.ensure((size_t)lp::kMaxDet * 2));
     LP_CUDA(c, c->counters.ensure(LP_NCOUNTERS));
     LP_CUDA(c, c->work.ensure(1));
+    LP_CUDA(c, c->grad.ensure((size_t)lp::kMaxDet * lp::kGradRegions * 5));
     return LP_OK;
 }
 
@@ -217,6 +224,7 @@ int zero_tallies(lp_ctx *c)
     LP_CUDA(c, cudaMemsetAsync(c->region.p, 0, lp::kMaxMedia * 8, s));
     LP_CUDA(c, cudaMemsetAsync(c->det.p, 0, lp::kMaxDet * 2 * 8, s));
     LP_CUDA(c, cudaMemsetAsync(c->counters.p, 0, LP_NCOUNTERS * 8, s));
+    LP_CUDA(c, cudaMemsetAsync(c->grad.p, 0, (size_t)lp::kMaxDet * lp::kGradRegions * 5 * 8, s));
     return LP_OK;
 }
 
@@ -392,6 +400,7 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     }
     P.exit_rec = c->exit_cap > 0 ? c->exit_rec.p : nullptr;
     P.exit_cap = c->exit_cap;
+    P.grad = c->grad_on ? c->grad.p : nullptr;
     P.work = c->work.p;
     const bool grid = c->grid_max_cells > 0 && c->cell_word.p && !c->grid_dirty;
     P.cell_word = grid ? c->cell_word.p : nullptr;
@@ -722,6 +731,102 @@ int lp_set_safety_grid(lp_ctx *c, int64_t max_cells)
     return LP_OK;
 }
 
+int lp_set_gradient(lp_ctx *c, int enable)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_gradient: ctx is NULL");
+    c->grad_on = enable != 0;
+    return LP_OK;
+}
+
+int lp_get_gradient(lp_ctx *c, lp_gradient *out)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_gradient: NULL argument");
+    if (!c->grad.p || !c->counters.p || !c->det.p) return fail(c, LP_ERR_STATE, "lp_get_gradient: nothing has run");
+    const int D = (int)c->det_r.size() / 2, R = c->n_media;
+    if (R > lp::kGradRegions) return fail(c, LP_ERR_RANGE, "lp_get_gradient: %d regions (at most %d)", R,
+                                          lp::kGradRegions);
+    LP_CUDA(c, cudaSetDevice(c->device));
+    std::vector<uint64_t> det((size_t)std::max(D, 1) * 2), cnt(LP_NCOUNTERS);
+    c->h_grad.assign((size_t)std::max(D * R, 1) * 5, 0.0);
+    cudaStream_t s = c->stream;
+    if (D > 0) {
+        LP_CUDA(c, cudaMemcpyAsync(c->h_grad.data(), c->grad.p, (size_t)D * R * 5 * 8, cudaMemcpyDeviceToHost, s));
+        LP_CUDA(c, cudaMemcpyAsync(det.data(), c->det.p, (size_t)D * 2 * 8, cudaMemcpyDeviceToHost, s));
+    }
+    LP_CUDA(c, cudaMemcpyAsync(cnt.data(), c->counters.p, LP_NCOUNTERS * 8, cudaMemcpyDeviceToHost, s));
+    LP_CUDA(c, cudaStreamSynchronize(s));
+    const double N = (double)cnt[LP_C_PHOTONS], f = (double)c->factor;
+    c->g_signal.assign((size_t)D, 0.0);
+    c->g_signal_se.assign((size_t)D, 0.0);
+    c->g_mua.assign((size_t)D * R, 0.0);
+    c->g_mus.assign((size_t)D * R, 0.0);
+    c->g_mua_se.assign((size_t)D * R, 0.0);
+    c->g_mus_se.assign((size_t)D * R, 0.0);
+    // standard error of the mean of per-photon values x (0 for photons not scored)
+    auto se = [N](double sx, double sxx) { return N > 1 ? std::sqrt(std::max(sxx / N - (sx / N) * (sx / N), 0.0) / N) : 0.0; };
+    for (int d = 0; d < D && N > 0; ++d) {
+        const double s1 = (double)det[2 * d] / LP_FIX_ONE, s2 = (double)det[2 * d + 1] / LP_FIX_ONE;
+        c->g_signal[d] = s1 / N;
+        c->g_signal_se[d] = se(s1, s2);
+        for (int r = 0; r < R; ++r) {
+            const double *g = &c->h_grad[5 * ((size_t)d * R + r)];
+            const double A = g[0], B = g[1], AA = g[2], BB = g[3], AB = g[4];
+            const size_t i = (size_t)d * R + r;
+            c->g_mua[i] = -A / f / N;
+            c->g_mua_se[i] = se(-A / f, AA / (f * f));
+            const double mus = (double)c->nmuasg[4 * r + 2];
+            if (mus > 0.0) {
+                const double sx = B / mus - A / f;
+                const double sxx = BB / (mus * mus) + AA / (f * f) - 2.0 * AB / (mus * f);
+                c->g_mus[i] = sx / N;
+                c->g_mus_se[i] = se(sx, sxx);
+            }
+        }
+    }
+    out->n_det = D;
+    out->n_media = R;
+    out->n_photons = (int64_t)cnt[LP_C_PHOTONS];
+    out->signal = c->g_signal.data();
+    out->signal_se = c->g_signal_se.data();
+    out->d_mua = c->g_mua.data();
+    out->d_mus = c->g_mus.data();
+    out->d_mua_se = c->g_mua_se.data();
+    out->d_mus_se = c->g_mus_se.data();
+    c->d2h_bytes = (int64_t)(D * R * 5 + D * 2 + LP_NCOUNTERS) * 8;
+    return LP_OK;
+}
+
+int lp_forward(lp_ctx *c, int64_t first, int64_t n, double *signal)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_forward: ctx is NULL");
+    c->grad_on = true;
+    int r = lp_zero_tallies(c);
+    if (r) return r;
+    if ((r = lp_run(c, first, n))) return r;
+    lp_gradient g;
+    if ((r = lp_get_gradient(c, &g))) return r;
+    if (signal)
+        for (int d = 0; d < g.n_det; ++d) signal[d] = g.signal[d];
+    return LP_OK;
+}
+
+int lp_backward(lp_ctx *c, const double *grad_signal, double *grad_mua, double *grad_mus)
+{
+    if (!c || !grad_signal || !grad_mua || !grad_mus) return fail(c, LP_ERR_INVALID, "lp_backward: NULL argument");
+    const int R = c->n_media, D = (int)c->g_signal.size();
+    if ((int64_t)c->g_mua.size() != (int64_t)D * R) return fail(c, LP_ERR_STATE, "lp_backward: no lp_forward before");
+    for (int r = 0; r < R; ++r) {
+        double a = 0.0, b = 0.0;
+        for (int d = 0; d < D; ++d) {
+            a += grad_signal[d] * c->g_mua[(size_t)d * R + r];
+            b += grad_signal[d] * c->g_mus[(size_t)d * R + r];
+        }
+        grad_mua[r] = a;
+        grad_mus[r] = b;
+    }
+    return LP_OK;
+}
+
 int lp_set_cell_lists(lp_ctx *c, int enable)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_cell_lists: ctx is NULL");
@@ -755,11 +860,19 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
     int r = upload(c);
     if (r) return r;
     if (n == 0) return LP_OK;
+    if (c->grad_on && c->n_media > lp::kGradRegions)
+        return fail(c, LP_ERR_RANGE, "lp_run: differentiation supports at most %d regions (%d set)",
+                    lp::kGradRegions, c->n_media);
     int nodes_smem, tris_smem;
     smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
     const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     int per_sm = 0;
-    LP_CUDA(c, c->exact ? lp::transport_occupancy_exact(smem, &per_sm) : lp::transport_occupancy_fast(smem, &per_sm));
+    if (c->grad_on)
+        LP_CUDA(c, c->exact ? lp::transport_occupancy_exact_grad(smem, &per_sm)
+                            : lp::transport_occupancy_fast_grad(smem, &per_sm));
+    else
+        LP_CUDA(c, c->exact ? lp::transport_occupancy_exact(smem, &per_sm)
+                            : lp::transport_occupancy_fast(smem, &per_sm));
     if (per_sm < 1) return fail(c, LP_ERR_CUDA, "lp_run: transport kernel does not fit on an SM");
     KParams P;
     fill_params(c, P, first, n, nodes_smem, tris_smem);

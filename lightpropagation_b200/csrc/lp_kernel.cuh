@@ -14,6 +14,7 @@ namespace lp {
 constexpr int kMaxMedia = 64;
 constexpr int kMaxDet = 32;
 constexpr int kStackDepth = 64;
+constexpr int kGradRegions = 8;      // regions a differentiated run may have
 constexpr float kNoHit = 10000.0f;   // FindTriangleInPath's initial distance (.cl:1042)
 
 struct Medium {
@@ -66,6 +67,11 @@ struct KParams {
     float det_lo[kMaxDet], det_hi[kMaxDet];
     float *exit_rec;
     int64_t exit_cap;
+    // differentiation (null: off): per (ring detector d, region r), over the photons
+    // scored in ring d with surface weight s, the sums of a = s * L_r and b = s * k_r,
+    // where L_r is the photon's path length and k_r its number of interactions in
+    // region r: grad[5 * (d * n_media + r) + {0..4}] = sum a, sum b, sum a^2, sum b^2, sum a b
+    double *grad;
     // cell grid over the mesh bounds (cubic cells of size 1 / g_inv_h), one word per cell:
     //   kCellEmpty set:   no triangle touches the cell; bits 0-15 hold a lower bound of
     //                     the distance from any point of the cell to the nearest

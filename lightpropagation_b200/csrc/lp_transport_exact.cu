@@ -12,7 +12,12 @@ cudaError_t launch_transport_exact(const KParams &P, int grid, int smem, cudaStr
 
 cudaError_t transport_occupancy_exact(int smem, int *blocks_per_sm)
 {
-    return transport_occupancy_t<true>(smem, blocks_per_sm);
+    return transport_occupancy_t<true, false>(smem, blocks_per_sm);
+}
+
+cudaError_t transport_occupancy_exact_grad(int smem, int *blocks_per_sm)
+{
+    return transport_occupancy_t<true, true>(smem, blocks_per_sm);
 }
 
 __global__ void __launch_bounds__(kBlock) query_kernel(const __grid_constant__ KParams P, int64_t n,

@@ -11,7 +11,12 @@ cudaError_t launch_transport_fast(const KParams &P, int grid, int smem, cudaStre
 
 cudaError_t transport_occupancy_fast(int smem, int *blocks_per_sm)
 {
-    return transport_occupancy_t<false>(smem, blocks_per_sm);
+    return transport_occupancy_t<false, false>(smem, blocks_per_sm);
+}
+
+cudaError_t transport_occupancy_fast_grad(int smem, int *blocks_per_sm)
+{
+    return transport_occupancy_t<false, true>(smem, blocks_per_sm);
 }
 
 }  // namespace lp

@@ -44,6 +44,15 @@ struct Photon {
     uint32_t flags;          // bit0 traversedFetalTissue, bit1 roulette, bits 2-3 exit kind
     unsigned long long region_acc;
     int64_t pid;
+    float seg_len;           // differentiation: path length and interactions in the
+    uint32_t seg_k;          // current region since the photon entered it
+};
+
+// Per-photon, per-region path lengths and interaction counts of a differentiated run
+// (thread-local, indexed by region id).
+struct GradAcc {
+    float L[kGradRegions];
+    uint32_t k[kGradRegions];
 };
 enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2 };
 enum : uint32_t { EXIT_NONE = 0, EXIT_SURF = 1, EXIT_SURF_FETAL = 2, EXIT_TRANS = 3 };
@@ -169,8 +178,29 @@ __device__ __forceinline__ void add_fix(unsigned long long *a, float w)
     if (f) atomicAdd(a, f);
 }
 
+// Differentiation: the photon scored surface weight s in ring d.  With path density
+// prod_r mus_r^k_r exp(-(mua_r + mus_r) L_r / factor) times the albedo weights, the
+// score's derivatives are s * (-L_r / factor) for mua_r and s * (k_r / mus_r - L_r / factor)
+// for mus_r (perturbation Monte Carlo, Hayakawa et al., Opt. Lett. 26, 2001); the
+// kernel accumulates the moments of s L_r and s k_r, the host forms the derivatives.
+static __device__ __noinline__ void score_gradient(const KParams &P, const GradAcc &ga, int d, float s)
+{
+    double *g = P.grad + 5 * (int64_t)d * P.n_media;
+    for (int r = 0; r < P.n_media; ++r) {
+        const double a = (double)s * (double)ga.L[r];
+        const double b = (double)s * (double)ga.k[r];
+        if (a == 0.0 && b == 0.0) continue;
+        atomicAdd(g + 5 * r + 0, a);
+        atomicAdd(g + 5 * r + 1, b);
+        atomicAdd(g + 5 * r + 2, a * a);
+        atomicAdd(g + 5 * r + 3, b * b);
+        atomicAdd(g + 5 * r + 4, a * b);
+    }
+}
+
 // Exit record binning of CalculatePropagation.cpp:1553-1626 plus radial bins and rings.
-static __device__ __noinline__ void finish_photon(const KParams &P, const Photon &ph)
+template <bool Grad>
+static __device__ __noinline__ void finish_photon(const KParams &P, const Photon &ph, const GradAcc *ga)
 {
     const V3 v = v3(ph.vx, ph.vy, ph.vz), nv = v3(ph.nvx, ph.nvy, ph.nvz);
     const float alpha = fabsf(acosf(dot3(v, nv)));
@@ -222,6 +252,7 @@ static __device__ __noinline__ void finish_photon(const KParams &P, const Photon
             if (rho >= P.det_lo[k] && rho < P.det_hi[k]) {
                 add_fix(P.det + 2 * k, s);
                 add_fix(P.det + 2 * k + 1, s * s);
+                if (Grad) score_gradient(P, *ga, k, s);
             }
         }
     }
@@ -261,13 +292,15 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
     ph.flags = F_ROULETTE;
     ph.region_acc = 0;
     ph.pid = pid;
+    ph.seg_len = 0.0f;
+    ph.seg_k = 0;
 }
 
 // One iteration of the reference's do-while loop.  Returns false when the photon ends.
-template <bool Exact>
+template <bool Exact, bool Grad>
 __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
                                             unsigned long long *s_region, unsigned long long *s_cnt,
-                                            Photon &ph, Counters &cnt)
+                                            Photon &ph, Counters &cnt, GradAcc *ga)
 {
     EventRng rng;
     rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
@@ -394,6 +427,14 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             if (newID != prev) {
                 if (ph.region_acc) atomicAdd(s_region + prev, ph.region_acc);
                 ph.region_acc = 0;
+                if (Grad) {
+                    ga->L[prev] += ph.seg_len + thit;
+                    ga->k[prev] += ph.seg_k;
+                    ph.seg_len = 0.0f;
+                    ph.seg_k = 0;
+                }
+            } else if (Grad) {
+                ph.seg_len += thit;
             }
         }
     } else {
@@ -402,6 +443,10 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.py = ph.py + step * ph.vy;
         ph.pz = ph.pz + step * ph.vz;
         ph.refTri = -1;
+        if (Grad) {
+            ph.seg_len += step;
+            ph.seg_k++;
+        }
         if (m.absorbs) {
             ph.absorbed = ph.w * m.alb;
             ph.w -= ph.absorbed;
@@ -516,7 +561,7 @@ __device__ __forceinline__ MeshView stage_mesh(const KParams &P, unsigned char *
     return M;
 }
 
-template <bool Exact>
+template <bool Exact, bool Grad>
 __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_constant__ KParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -537,6 +582,7 @@ __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_const
     Counters cnt = {};
     uint32_t photons = 0;
     Photon ph;
+    GradAcc ga;
     bool alive = false;
     bool exhausted = false;
     for (;;) {
@@ -551,15 +597,25 @@ __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_const
                 const unsigned long long idx = base + __popc(need & lt_mask);
                 if (idx < (unsigned long long)P.n) {
                     start_photon(P, ph, P.first + (int64_t)idx);
+                    if (Grad) {
+                        for (int r = 0; r < P.n_media; ++r) {
+                            ga.L[r] = 0.0f;
+                            ga.k[r] = 0;
+                        }
+                    }
                     alive = true;
                 }
             }
         }
         if (!__any_sync(0xffffffffu, alive)) break;
         if (alive) {
-            if (!step_photon<Exact>(P, M, s_media, s_region, s_cnt, ph, cnt)) {
+            if (!step_photon<Exact, Grad>(P, M, s_media, s_region, s_cnt, ph, cnt, &ga)) {
                 if (ph.region_acc) atomicAdd(s_region + ph.curr, ph.region_acc);
-                finish_photon(P, ph);
+                if (Grad) {
+                    ga.L[ph.curr] += ph.seg_len;
+                    ga.k[ph.curr] += ph.seg_k;
+                }
+                finish_photon<Grad>(P, ph, Grad ? &ga : nullptr);
                 photons++;
                 alive = false;
             }
@@ -591,19 +647,22 @@ __global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_const
         if (s_region[i]) atomicAdd(P.region + i, s_region[i]);
 }
 
+// P.grad selects the differentiating instantiation.
 template <bool Exact>
 cudaError_t launch_transport_t(const KParams &P, int grid, int smem, cudaStream_t s)
 {
-    transport_kernel<Exact><<<grid, kBlock, smem, s>>>(P);
+    if (P.grad) transport_kernel<Exact, true><<<grid, kBlock, smem, s>>>(P);
+    else transport_kernel<Exact, false><<<grid, kBlock, smem, s>>>(P);
     return cudaGetLastError();
 }
 
-template <bool Exact>
+template <bool Exact, bool Grad>
 cudaError_t transport_occupancy_t(int smem, int *blocks_per_sm)
 {
-    cudaError_t e = cudaFuncSetAttribute(transport_kernel<Exact>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(transport_kernel<Exact, Grad>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<Exact>, kBlock, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<Exact, Grad>, kBlock, smem);
 }
 
 }  // namespace lp

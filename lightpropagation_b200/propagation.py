@@ -49,6 +49,8 @@ class Simulation:
         self._h = h
         self._L = L
         self.device = device
+        self._n_media = 0
+        self._rings = np.zeros((0, 2), np.float32)
 
     # -- lifetime
     def close(self):
@@ -82,6 +84,7 @@ class Simulation:
     def set_media(self, nmuasg):
         a = _f32(nmuasg)
         self._ck(self._L.lp_set_media(self._h, a.size // 4, N.fptr(a)))
+        self._n_media = a.size // 4
 
     def set_source(self, p_start, v_start, ep0xyz, v_occ=None):
         p, v, e = _f32(p_start, 3), _f32(v_start), _f32(ep0xyz, 12)
@@ -103,6 +106,7 @@ class Simulation:
         dr = _f32(det_r if det_r is not None else np.zeros((0, 2)))
         self._ck(self._L.lp_set_extra_tallies(self._h, N.iptr(vn), N.fptr(vd), int(n_rbins), float(rbin_dr),
                                               dr.size // 2, N.fptr(dr)))
+        self._rings = dr.reshape(-1, 2).copy()
 
     def set_arithmetic(self, exact: bool):
         """exact=True: the reference kernel's operation order; False (default): fast."""
@@ -111,6 +115,45 @@ class Simulation:
     def set_safety_grid(self, max_cells: int):
         """Cells of the query-skipping safety grid (0 disables it; results are unchanged)."""
         self._ck(self._L.lp_set_safety_grid(self._h, int(max_cells)))
+
+    # -- differentiation (lp_set_gradient / lp_forward / lp_backward)
+    def set_gradient(self, enable: bool):
+        """Accumulate d(ring signal)/d(mua, mus) sums in the following runs."""
+        self._ck(self._L.lp_set_gradient(self._h, 1 if enable else 0))
+
+    def gradient(self) -> dict:
+        """Ring signals S_d and dS_d/dmua_r, dS_d/dmus_r with standard errors."""
+        g = N.Gradient()
+        self._ck(self._L.lp_get_gradient(self._h, C.byref(g)))
+        D, R = g.n_det, g.n_media
+
+        def arr(p, shape):
+            n = int(np.prod(shape))
+            return np.ctypeslib.as_array(p, shape=(n,)).copy().reshape(shape) if n else np.zeros(shape)
+
+        return {"n_photons": int(g.n_photons), "signal": arr(g.signal, (D,)), "signal_se": arr(g.signal_se, (D,)),
+                "d_mua": arr(g.d_mua, (D, R)), "d_mus": arr(g.d_mus, (D, R)),
+                "d_mua_se": arr(g.d_mua_se, (D, R)), "d_mus_se": arr(g.d_mus_se, (D, R))}
+
+    def forward(self, n: int, first: int = 0) -> np.ndarray:
+        """Zero the tallies, trace photons [first, first + n) with differentiation on and
+        return the ring signals."""
+        d = max(1, len(self.geometry_rings()))
+        out = np.zeros(d, np.float64)
+        self._ck(self._L.lp_forward(self._h, int(first), int(n), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out[:len(self.geometry_rings())]
+
+    def backward(self, grad_signal):
+        """Vector-Jacobian product of the last forward: (grad_mua, grad_mus) per region."""
+        g = np.ascontiguousarray(grad_signal, np.float64)
+        r = self._n_media
+        gm, gs = np.zeros(r, np.float64), np.zeros(r, np.float64)
+        dp = C.POINTER(C.c_double)
+        self._ck(self._L.lp_backward(self._h, g.ctypes.data_as(dp), gm.ctypes.data_as(dp), gs.ctypes.data_as(dp)))
+        return gm, gs
+
+    def geometry_rings(self) -> np.ndarray:
+        return self._rings
 
     def set_cell_lists(self, enable: bool):
         """Cells touched by triangles list them for short-step queries (default on;

@@ -452,7 +452,7 @@ static inline int trunc_sat(double x)
 }
 
 /* Host binning of one exit record (CalculatePropagation.cpp:1553-1626). */
-static void bin_exit(const ctx_t *C, lpo_tallies *T, const float rec[8])
+static void bin_exit(const ctx_t *C, lpo_tallies *T, const float rec[8], const double *L, const int64_t *K)
 {
     const lpo_problem *P = C->P;
     const lpo_geometry *g = &C->g;
@@ -492,6 +492,17 @@ static void bin_exit(const ctx_t *C, lpo_tallies *T, const float rec[8])
             if (rho >= P->det_r[2 * d] && rho < P->det_r[2 * d + 1]) {
                 tally_add(&T->det[2 * d], s);
                 tally_add(&T->det[2 * d + 1], s * s);
+                if (T->grad && L) {
+                    for (int r = 0; r < P->n_media; r++) {
+                        double a = (double)s * L[r], b = (double)s * (double)K[r];
+                        double *g = T->grad + 5 * ((int64_t)d * P->n_media + r);
+                        g[0] += a;
+                        g[1] += b;
+                        g[2] += a * a;
+                        g[3] += b * b;
+                        g[4] += a * b;
+                    }
+                }
             }
         }
     }
@@ -535,6 +546,14 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
     int roulette = 1;
     int64_t steps = 0;
     uint64_t region_acc = 0;
+    /* path length and interactions per region, for the perturbation-MC sums */
+    double L[LPO_MAX_MEDIA];
+    int64_t K[LPO_MAX_MEDIA];
+    const int track = T->grad != NULL && P->n_media <= LPO_MAX_MEDIA;
+    if (track) {
+        memset(L, 0, sizeof L);
+        memset(K, 0, sizeof K);
+    }
     do {
         float pp[3] = {ph.p.x, ph.p.y, ph.p.z}, vv[3] = {ph.v.x, ph.v.y, ph.v.z};
         int triID = lpo_find_triangle(P->tri, P->n_tri, ph.refTri, pp, vv, &ph.steptoboundary);
@@ -561,6 +580,7 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
                 T->counters[LPO_C_MISS]++;
                 ph.w = 0;
             } else {
+                if (track) L[curr] += ph.steptoboundary;
                 int inner = P->med[2 * triID], outer = P->med[2 * triID + 1];
                 nv = normalize(ld3(P->nrm, triID));
                 const float *nxt = (curr == outer) ? nm + 4 * inner : nm + 4 * outer;
@@ -583,6 +603,10 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
             T->counters[LPO_C_SCATTER]++;
             ph.p = add(ph.p, scl(ph.stepsize, ph.v));
             ph.refTri = -1;
+            if (track) {
+                L[curr] += ph.stepsize;
+                K[curr]++;
+            }
             /* Absorb (.cl:841-847) */
             if (cur[1] > 0.0f && cur[2] > 0.0f) {
                 ph.absorbed = ph.w * (cur[1] / (cur[1] + cur[2]));
@@ -631,7 +655,7 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
     rec[6] = alpha;
     rec[7] = radius;
     if (rec_out) memcpy(rec_out, rec, sizeof rec);
-    bin_exit(C, T, rec);
+    bin_exit(C, T, rec, track ? L : NULL, track ? K : NULL);
 }
 
 static void ctx_init(ctx_t *C, const lpo_problem *P)
@@ -737,6 +761,7 @@ int lpo_run(const lpo_problem *P, int64_t first, int64_t n, int nthreads,
         w->T.rbins = (T->rbins && P->n_rbins > 0) ? (uint64_t *)calloc((size_t)P->n_rbins * 2, 8) : NULL;
         w->T.region = T->region ? (uint64_t *)calloc((size_t)P->n_media, 8) : NULL;
         w->T.det = (T->det && P->n_det > 0) ? (uint64_t *)calloc((size_t)P->n_det * 2, 8) : NULL;
+        w->T.grad = (T->grad && P->n_det > 0) ? (double *)calloc((size_t)P->n_det * P->n_media * 5, 8) : NULL;
         w->T.exit_rec = NULL;
         w->T.rz_ref = NULL; /* the reference-layout buffer is only kept in the sequential mode */
         if (t > 0) pthread_create(&th[t], NULL, worker_main, w);
@@ -752,9 +777,11 @@ int lpo_run(const lpo_problem *P, int64_t first, int64_t n, int nthreads,
         merge(T->rbins, w->T.rbins, (size_t)P->n_rbins * 2);
         merge(T->region, w->T.region, (size_t)P->n_media);
         merge(T->det, w->T.det, (size_t)P->n_det * 2);
+        if (T->grad && w->T.grad)
+            for (size_t k = 0; k < (size_t)P->n_det * P->n_media * 5; k++) T->grad[k] += w->T.grad[k];
         for (int k = 0; k < LPO_NCOUNTERS; k++) T->counters[k] += w->T.counters[k];
         free(w->T.sft); free(w->T.rtd); free(w->T.rz); free(w->T.vox);
-        free(w->T.rbins); free(w->T.region); free(w->T.det);
+        free(w->T.rbins); free(w->T.region); free(w->T.det); free(w->T.grad);
     }
     free(W);
     free(th);

@@ -46,6 +46,7 @@ enum { LPO_RNG_RAN3_SHARED = 0, LPO_RNG_RAN3_PHOTON = 1, LPO_RNG_PHILOX = 2 };
 #define LPO_COMPAT_AXIS_NORMAL    0x2u /* normal := +-eZ within 0.01 of the axis, .cl:1493  */
 #define LPO_COMPAT_SIGNED_FRESNEL 0x4u /* Fresnel with signed cos(incidence), .cl:889-896   */
 #define LPO_COMPAT_ALL            0x7u
+#define LPO_MAX_MEDIA             64   /* regions the perturbation-MC sums can track */
 
 /* counters[] slots */
 enum {
@@ -121,6 +122,13 @@ typedef struct lpo_tallies {
     float *rz_ref;      /* optional reference-layout r-z buffer, see lpo_rz_ref_layout  */
     int64_t rz_ref_cells;   /* cells (3 floats each) in rz_ref                          */
     int64_t rz_ref_offset;  /* cell index of the reference's cell 0 inside rz_ref       */
+    /* optional perturbation-MC sums [n_det][n_media][5] (FP64): over the photons
+     * scored in ring d with surface weight s, with L_r / k_r the photon's path length /
+     * interaction count in region r: sum s L_r, sum s k_r, sum (s L_r)^2,
+     * sum (s k_r)^2, sum (s L_r)(s k_r).  The derivative of the ring signal
+     * (mean s per launched photon) is -sum s L_r / (factor N) for mua_r and
+     * (sum s k_r / mus_r - sum s L_r / factor) / N for mus_r. */
+    double *grad;
 } lpo_tallies;
 
 /* Philox4x32-10 block function (Salmon et al., SC'11). */

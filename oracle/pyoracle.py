@@ -61,7 +61,7 @@ class Tallies(C.Structure):
         ("sft", _up), ("rtd", _up), ("rz", _up), ("vox", _up), ("rbins", _up),
         ("region", _up), ("det", _up), ("counters", C.c_uint64 * NCOUNTERS),
         ("exit_rec", _fp), ("rz_ref", _fp), ("rz_ref_cells", C.c_int64),
-        ("rz_ref_offset", C.c_int64),
+        ("rz_ref_offset", C.c_int64), ("grad", C.POINTER(C.c_double)),
     ]
 
 
@@ -211,6 +211,20 @@ class Result:
     rz_ref: Optional[np.ndarray] = None
     ran3_state: Optional[np.ndarray] = None
     ran3_inext: Optional[np.ndarray] = None
+    grad: Optional[np.ndarray] = None       # [n_det, n_media, 5] perturbation-MC sums
+
+
+def gradient(res: Result, case: "Case", n: int):
+    """Ring signals and their derivatives from the perturbation-MC sums of a run of n
+    photons (see lpo_tallies.grad): (S [D], dS/dmua [D, R], dS/dmus [D, R])."""
+    s = res.det[:, 0].astype(np.float64) / 2.0 ** 32 / n
+    g = res.grad
+    f = float(case.factor)
+    mus = np.asarray(case.nmuasg, np.float64)[:, 2]
+    d_mua = -g[:, :, 0] / f / n
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d_mus = np.where(mus > 0, (g[:, :, 1] / mus - g[:, :, 0] / f) / n, 0.0)
+    return s, d_mua, d_mus
 
 
 def run(case: Case, n: int, first: int = 0, rng_mode=RNG_PHILOX, seed=0x4C50,
@@ -231,6 +245,9 @@ def run(case: Case, n: int, first: int = 0, rng_mode=RNG_PHILOX, seed=0x4C50,
     T = Tallies()
     T.sft, T.rtd, T.rz, T.vox = uptr(sft), uptr(rtd), uptr(rz), uptr(vox)
     T.rbins, T.region, T.det = uptr(rbins), uptr(region), uptr(det)
+    grad = np.zeros((max(ndet, 1), case.nmuasg.shape[0], 5), np.float64)
+    if ndet:
+        T.grad = grad.ctypes.data_as(C.POINTER(C.c_double))
     rec = None
     if exit_records:
         rec = np.zeros((n, 8), np.float32)
@@ -254,7 +271,7 @@ def run(case: Case, n: int, first: int = 0, rng_mode=RNG_PHILOX, seed=0x4C50,
                   C.byref(T))
     counters = {k: int(T.counters[i]) for i, k in enumerate(COUNTER_NAMES)}
     return Result(sft, rtd, rz, vox[:nv] if nv else vox[:0], rbins[:case.n_rbins], region,
-                  det[:ndet], counters, rec, rzref, st, ix)
+                  det[:ndet], counters, rec, rzref, st, ix, grad[:ndet])
 
 
 def ran3_init(seed: int):
