@@ -168,6 +168,48 @@ int lp_forward(lp_ctx *ctx, int64_t first, int64_t n, double *signal);
  * entries each. */
 int lp_backward(lp_ctx *ctx, const double *grad_signal, double *grad_mua, double *grad_mus);
 
+/* ---- Batches (no reference counterpart) -----------------------------------------
+ * Many transport instances in one persistent launch, replayed as a CUDA graph.  An
+ * instance is one of the batch's contexts (its mesh, source, tally layout and run
+ * parameters as set on that lp_ctx) with its own optical properties, photon range and
+ * tallies.  The reference traces one problem per program run
+ * (CalculatePropagation.cpp:1389-1759); here wavelengths x optical-property draws x
+ * meshes with uneven budgets share the GPU and drain once.  Each instance's tallies
+ * equal, bit for bit, those of lp_run on its context with its media and photon range.
+ * All contexts must live on the same device and share one tally layout. */
+#define LP_BATCH_MAX_MEDIA 8
+typedef struct lp_instance {
+    int32_t context;                          /* index into the batch's contexts         */
+    int32_t n_media;                          /* regions, at most LP_BATCH_MAX_MEDIA      */
+    float nmuasg[4 * LP_BATCH_MAX_MEDIA];     /* n, mua, mus, g per region                */
+    int64_t first;                            /* first photon id                          */
+    int64_t n_photons;
+} lp_instance;
+typedef struct lp_batch lp_batch;
+/* ctxs: n_ctx configured contexts (not owned; they must outlive the batch). */
+int lp_batch_create(lp_batch **out, int32_t n_ctx, lp_ctx *const *ctxs);
+void lp_batch_destroy(lp_batch *b);
+const char *lp_batch_last_error(const lp_batch *b);
+int lp_batch_set_instances(lp_batch *b, int32_t n_inst, const lp_instance *inst);
+/* Differentiation for every instance (see lp_set_gradient). */
+int lp_batch_set_gradient(lp_batch *b, int enable);
+/* Launch configuration: -1 (default) autotunes on the first run; 0..count-1 fixes one. */
+int lp_batch_config_count(void);
+int lp_batch_config_info(int32_t config, int32_t *block, int32_t *min_blocks, int32_t *stack);
+int lp_batch_set_config(lp_batch *b, int32_t config);
+/* Autotuner: time every eligible configuration on the current instances with the
+ * budgets scaled to about `photons` in total, keep the fastest.  ns_per_photon (may
+ * be NULL) receives lp_batch_config_count() values, device nanoseconds per photon
+ * (< 0: configuration not eligible for these meshes). */
+int lp_batch_autotune(lp_batch *b, int64_t photons, int32_t *best, double *ns_per_photon);
+/* Zero all instance tallies and trace every instance (one graph launch). */
+int lp_batch_run(lp_batch *b);
+int lp_batch_last_ms(const lp_batch *b, float *ms);
+/* Ring signals S_d per instance and their relative standard errors, [n_inst][n_det]. */
+int lp_batch_ring_signals(lp_batch *b, double *signal, double *rel_err);
+int lp_batch_get_tallies(lp_batch *b, int32_t inst, lp_tallies *out);
+int lp_batch_get_gradient(lp_batch *b, int32_t inst, lp_gradient *out);
+
 /* Whether cells touched by triangles list them (1, default) or hold no information
  * (0: every query that the safety bound does not skip descends the BVH).  Results are
  * identical either way; lp_query_triangles follows the same setting. */

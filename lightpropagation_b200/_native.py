@@ -67,8 +67,15 @@ class NoAllocArgs(C.Structure):
 
 NOALLOC_MAX_TRI, NOALLOC_MAX_MEDIA = 4096, 64
 GRAD_MAX_REGIONS = 8
+BATCH_MAX_MEDIA = 8
 
 _dp = C.POINTER(C.c_double)
+
+
+class Instance(C.Structure):
+    """lp_instance: one transport problem of a batch."""
+    _fields_ = [("context", C.c_int32), ("n_media", C.c_int32), ("nmuasg", C.c_float * (4 * BATCH_MAX_MEDIA)),
+                ("first", C.c_int64), ("n_photons", C.c_int64)]
 
 
 class Gradient(C.Structure):
@@ -117,6 +124,20 @@ _SIGS = {
     "lp_get_device_tallies": ([C.c_void_p, C.POINTER(DeviceTallies)], C.c_int),
     "lp_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
     "lp_run_noalloc": ([C.POINTER(NoAllocArgs), C.c_void_p], C.c_int),
+    "lp_batch_config_count": ([], C.c_int),
+    "lp_batch_config_info": ([C.c_int32, _ip, _ip, _ip], C.c_int),
+    "lp_batch_create": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
+    "lp_batch_destroy": ([C.c_void_p], None),
+    "lp_batch_last_error": ([C.c_void_p], C.c_char_p),
+    "lp_batch_set_instances": ([C.c_void_p, C.c_int32, C.POINTER(Instance)], C.c_int),
+    "lp_batch_set_gradient": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_batch_set_config": ([C.c_void_p, C.c_int32], C.c_int),
+    "lp_batch_autotune": ([C.c_void_p, C.c_int64, _ip, _dp], C.c_int),
+    "lp_batch_run": ([C.c_void_p], C.c_int),
+    "lp_batch_last_ms": ([C.c_void_p, _fp], C.c_int),
+    "lp_batch_ring_signals": ([C.c_void_p, _dp, _dp], C.c_int),
+    "lp_batch_get_tallies": ([C.c_void_p, C.c_int32, C.POINTER(Tallies)], C.c_int),
+    "lp_batch_get_gradient": ([C.c_void_p, C.c_int32, C.POINTER(Gradient)], C.c_int),
     "lp_set_gradient": ([C.c_void_p, C.c_int], C.c_int),
     "lp_get_gradient": ([C.c_void_p, C.POINTER(Gradient)], C.c_int),
     "lp_forward": ([C.c_void_p, C.c_int64, C.c_int64, _dp], C.c_int),
@@ -144,6 +165,12 @@ def lib():
 def check(rc: int, ctx=None) -> None:
     if rc != LP_OK:
         msg = lib().lp_last_error(ctx)
+        raise LPError(rc, msg.decode() if msg else "")
+
+
+def check_batch(rc: int, batch=None) -> None:
+    if rc != LP_OK:
+        msg = lib().lp_batch_last_error(batch)
         raise LPError(rc, msg.decode() if msg else "")
 
 

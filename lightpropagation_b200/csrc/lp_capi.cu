@@ -77,6 +77,61 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Ring signals and their derivatives formed from the device sums (see KParams::grad).
+struct GradOut {
+    std::vector<double> signal, signal_se, mua, mus, mua_se, mus_se;
+};
+
+// det: [D][2] fixed-point (sum s, sum s^2); gsum: [D][R][5]; N photons; per-photon values
+// are 0 for photons not scored, so each standard error is that of a mean over N.
+void form_gradient(const uint64_t *det, const double *gsum, double N, double factor, const float *nmuasg, int D,
+                   int R, GradOut &o)
+{
+    o.signal.assign((size_t)D, 0.0);
+    o.signal_se.assign((size_t)D, 0.0);
+    o.mua.assign((size_t)D * R, 0.0);
+    o.mus.assign((size_t)D * R, 0.0);
+    o.mua_se.assign((size_t)D * R, 0.0);
+    o.mus_se.assign((size_t)D * R, 0.0);
+    auto se = [N](double sx, double sxx) {
+        return N > 1 ? std::sqrt(std::max(sxx / N - (sx / N) * (sx / N), 0.0) / N) : 0.0;
+    };
+    const double f = factor;
+    for (int d = 0; d < D && N > 0; ++d) {
+        const double s1 = (double)det[2 * d] / LP_FIX_ONE, s2 = (double)det[2 * d + 1] / LP_FIX_ONE;
+        o.signal[d] = s1 / N;
+        o.signal_se[d] = se(s1, s2);
+        if (!gsum) continue;
+        for (int r = 0; r < R; ++r) {
+            const double *g = gsum + 5 * ((size_t)d * R + r);
+            const double A = g[0], B = g[1], AA = g[2], BB = g[3], AB = g[4];
+            const size_t i = (size_t)d * R + r;
+            o.mua[i] = -A / f / N;
+            o.mua_se[i] = se(-A / f, AA / (f * f));
+            const double mus = (double)nmuasg[4 * r + 2];
+            if (mus > 0.0) {
+                const double sx = B / mus - A / f;
+                const double sxx = BB / (mus * mus) + AA / (f * f) - 2.0 * AB / (mus * f);
+                o.mus[i] = sx / N;
+                o.mus_se[i] = se(sx, sxx);
+            }
+        }
+    }
+}
+
+void fill_gradient(const GradOut &o, int D, int R, int64_t n, lp_gradient *out)
+{
+    out->n_det = D;
+    out->n_media = R;
+    out->n_photons = n;
+    out->signal = o.signal.data();
+    out->signal_se = o.signal_se.data();
+    out->d_mua = o.mua.data();
+    out->d_mus = o.mus.data();
+    out->d_mua_se = o.mua_se.data();
+    out->d_mus_se = o.mus_se.data();
+}
+
 }  // namespace
 
 struct lp_ctx {
@@ -129,7 +184,8 @@ struct lp_ctx {
     // differentiation (lp_set_gradient / lp_forward / lp_backward)
     bool grad_on = false;
     DevBuf<double> grad;                  // [kMaxDet][kGradRegions][5], see KParams::grad
-    std::vector<double> h_grad, g_signal, g_signal_se, g_mua, g_mus, g_mua_se, g_mus_se;
+    std::vector<double> h_grad;
+    GradOut gout;
     // host copies of tallies
     std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
     float last_ms = 0.0f;
@@ -255,12 +311,12 @@ int upload_mesh(lp_ctx *c)
     return LP_OK;
 }
 
-int upload_media(lp_ctx *c)
+// Device media records (with the derived factors of the fast mode) from (n, mua, mus, g).
+void media_table(const float *nmuasg, int n_media, std::vector<Medium> &m)
 {
-    if (!c->media_dirty) return LP_OK;
-    std::vector<Medium> m((size_t)c->n_media);
-    for (int i = 0; i < c->n_media; ++i) {
-        const float *q = &c->nmuasg[4 * i];
+    m.assign((size_t)n_media, Medium{});
+    for (int i = 0; i < n_media; ++i) {
+        const float *q = &nmuasg[4 * i];
         m[i].n = q[0];
         m[i].mua = q[1];
         m[i].mus = q[2];
@@ -279,6 +335,13 @@ int upload_media(lp_ctx *c)
         m[i].hg_inv2g = g != 0.0f ? 1.0f / (2.0f * g) : 0.0f;
         m[i].pad_ = 0.0f;
     }
+}
+
+int upload_media(lp_ctx *c)
+{
+    if (!c->media_dirty) return LP_OK;
+    std::vector<Medium> m;
+    media_table(c->nmuasg.data(), c->n_media, m);
     LP_CUDA(c, c->media.ensure(lp::kMaxMedia));
     LP_CUDA(c, cudaMemcpyAsync(c->media.p, m.data(), m.size() * sizeof(Medium), cudaMemcpyHostToDevice,
                                c->stream));
@@ -755,43 +818,9 @@ int lp_get_gradient(lp_ctx *c, lp_gradient *out)
     }
     LP_CUDA(c, cudaMemcpyAsync(cnt.data(), c->counters.p, LP_NCOUNTERS * 8, cudaMemcpyDeviceToHost, s));
     LP_CUDA(c, cudaStreamSynchronize(s));
-    const double N = (double)cnt[LP_C_PHOTONS], f = (double)c->factor;
-    c->g_signal.assign((size_t)D, 0.0);
-    c->g_signal_se.assign((size_t)D, 0.0);
-    c->g_mua.assign((size_t)D * R, 0.0);
-    c->g_mus.assign((size_t)D * R, 0.0);
-    c->g_mua_se.assign((size_t)D * R, 0.0);
-    c->g_mus_se.assign((size_t)D * R, 0.0);
-    // standard error of the mean of per-photon values x (0 for photons not scored)
-    auto se = [N](double sx, double sxx) { return N > 1 ? std::sqrt(std::max(sxx / N - (sx / N) * (sx / N), 0.0) / N) : 0.0; };
-    for (int d = 0; d < D && N > 0; ++d) {
-        const double s1 = (double)det[2 * d] / LP_FIX_ONE, s2 = (double)det[2 * d + 1] / LP_FIX_ONE;
-        c->g_signal[d] = s1 / N;
-        c->g_signal_se[d] = se(s1, s2);
-        for (int r = 0; r < R; ++r) {
-            const double *g = &c->h_grad[5 * ((size_t)d * R + r)];
-            const double A = g[0], B = g[1], AA = g[2], BB = g[3], AB = g[4];
-            const size_t i = (size_t)d * R + r;
-            c->g_mua[i] = -A / f / N;
-            c->g_mua_se[i] = se(-A / f, AA / (f * f));
-            const double mus = (double)c->nmuasg[4 * r + 2];
-            if (mus > 0.0) {
-                const double sx = B / mus - A / f;
-                const double sxx = BB / (mus * mus) + AA / (f * f) - 2.0 * AB / (mus * f);
-                c->g_mus[i] = sx / N;
-                c->g_mus_se[i] = se(sx, sxx);
-            }
-        }
-    }
-    out->n_det = D;
-    out->n_media = R;
-    out->n_photons = (int64_t)cnt[LP_C_PHOTONS];
-    out->signal = c->g_signal.data();
-    out->signal_se = c->g_signal_se.data();
-    out->d_mua = c->g_mua.data();
-    out->d_mus = c->g_mus.data();
-    out->d_mua_se = c->g_mua_se.data();
-    out->d_mus_se = c->g_mus_se.data();
+    form_gradient(det.data(), c->h_grad.data(), (double)cnt[LP_C_PHOTONS], (double)c->factor, c->nmuasg.data(), D, R,
+                  c->gout);
+    fill_gradient(c->gout, D, R, (int64_t)cnt[LP_C_PHOTONS], out);
     c->d2h_bytes = (int64_t)(D * R * 5 + D * 2 + LP_NCOUNTERS) * 8;
     return LP_OK;
 }
@@ -813,13 +842,13 @@ int lp_forward(lp_ctx *c, int64_t first, int64_t n, double *signal)
 int lp_backward(lp_ctx *c, const double *grad_signal, double *grad_mua, double *grad_mus)
 {
     if (!c || !grad_signal || !grad_mua || !grad_mus) return fail(c, LP_ERR_INVALID, "lp_backward: NULL argument");
-    const int R = c->n_media, D = (int)c->g_signal.size();
-    if ((int64_t)c->g_mua.size() != (int64_t)D * R) return fail(c, LP_ERR_STATE, "lp_backward: no lp_forward before");
+    const int R = c->n_media, D = (int)c->gout.signal.size();
+    if ((int64_t)c->gout.mua.size() != (int64_t)D * R) return fail(c, LP_ERR_STATE, "lp_backward: no lp_forward before");
     for (int r = 0; r < R; ++r) {
         double a = 0.0, b = 0.0;
         for (int d = 0; d < D; ++d) {
-            a += grad_signal[d] * c->g_mua[(size_t)d * R + r];
-            b += grad_signal[d] * c->g_mus[(size_t)d * R + r];
+            a += grad_signal[d] * c->gout.mua[(size_t)d * R + r];
+            b += grad_signal[d] * c->gout.mus[(size_t)d * R + r];
         }
         grad_mua[r] = a;
         grad_mus[r] = b;
@@ -1093,6 +1122,510 @@ int lp_philox_blocks(int device, const uint32_t *ctr, const uint32_t *key, int64
     if (e == cudaSuccess) e = cudaMemcpy(out, b.p, (size_t)n * 16, cudaMemcpyDeviceToHost);
     b.release();
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_philox_blocks");
+    return LP_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ batches
+namespace lp {
+cudaError_t launch_batch(int config, bool grad, const BatchParams &B, int grid, cudaStream_t s);
+cudaError_t batch_occupancy(int config, bool grad, int *blocks_per_sm);
+int batch_config_count();
+int batch_config_info(int config, int *block, int *min_blocks, int *stack);
+}  // namespace lp
+
+struct lp_batch {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    std::vector<lp_ctx *> ctx;
+    std::vector<lp_instance> inst;
+    // elements of each tally per instance
+    size_t n_sft = 0, n_rtd = 0, n_rz = 0, n_vox = 0, n_rbins = 0, n_det = 0;
+    DevBuf<unsigned long long> sft, rtd, rz, vox, rbins, region, det, counters, claimed;
+    DevBuf<double> grad;
+    DevBuf<Medium> media;
+    DevBuf<KParams> params;
+    DevBuf<int32_t> frontier;
+    bool grad_on = false;
+    int config = -1;
+    int grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float last_ms = 0.0f;
+    std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det, h_cnt;
+    std::vector<double> h_grad;
+    GradOut gout;
+};
+
+namespace {
+
+int bfail(lp_batch *b, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    g_thread_error = buf;
+    return code;
+}
+
+#define LP_BCUDA(b, call)                                                        \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) return bfail(b, LP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e)); \
+    } while (0)
+
+void drop_graph(lp_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+size_t grad_stride(const lp_batch *b) { return std::max<size_t>(b->n_det, 1) * lp::kBatchMedia * 5; }
+
+// Per-instance parameters: the context's (mesh, source, tally layout, run parameters)
+// with the instance's media, photon range and tally slices.
+int upload_instances(lp_batch *b)
+{
+    const size_t I = b->inst.size();
+    std::vector<KParams> P(I);
+    std::vector<Medium> M(I * lp::kBatchMedia);
+    for (size_t i = 0; i < I; ++i) {
+        const lp_instance &in = b->inst[i];
+        lp_ctx *c = b->ctx[in.context];
+        KParams &p = P[i];
+        fill_params(c, p, in.first, in.n_photons, 0, 0);
+        std::vector<Medium> m;
+        media_table(in.nmuasg, in.n_media, m);
+        std::copy(m.begin(), m.end(), M.begin() + i * lp::kBatchMedia);
+        p.media = b->media.p + i * lp::kBatchMedia;
+        p.n_media = in.n_media;
+        p.Rsp = rspecular(in.nmuasg, in.n_media);
+        p.w0 = 1.0f - p.Rsp;
+        p.exitScale = (c->compat & LP_COMPAT_EXIT_RSP) ? (1 - p.Rsp) : 1.0f;
+        const float s = c->fiber_na / in.nmuasg[0];
+        p.src_cos_max = s < 1.0f ? std::sqrt(1.0f - s * s) : 0.0f;
+        p.sft = b->sft.p + i * b->n_sft;
+        p.rtd = b->rtd.p + i * b->n_rtd;
+        p.rz = b->rz.p + i * b->n_rz;
+        p.vox = b->vox.p + i * std::max<size_t>(b->n_vox, 1);
+        p.rbins = b->rbins.p + i * std::max<size_t>(b->n_rbins, 1);
+        p.region = b->region.p + i * lp::kBatchMedia;
+        p.det = b->det.p + i * std::max<size_t>(b->n_det, 1) * 2;
+        p.counters = b->counters.p + i * LP_NCOUNTERS;
+        p.grad = b->grad_on ? b->grad.p + i * grad_stride(b) : nullptr;
+        p.exit_rec = nullptr;
+        p.exit_cap = 0;
+        p.work = nullptr;
+    }
+    if (I) {
+        LP_BCUDA(b, cudaMemcpyAsync(b->params.p, P.data(), I * sizeof(KParams), cudaMemcpyHostToDevice, b->stream));
+        LP_BCUDA(b, cudaMemcpyAsync(b->media.p, M.data(), M.size() * sizeof(Medium), cudaMemcpyHostToDevice,
+                                    b->stream));
+        LP_BCUDA(b, cudaStreamSynchronize(b->stream));
+    }
+    return LP_OK;
+}
+
+// Zero the tallies and claim counters of all instances (enqueued on the batch stream).
+int enqueue_zero(lp_batch *b)
+{
+    const size_t I = b->inst.size();
+    cudaStream_t s = b->stream;
+    LP_BCUDA(b, cudaMemsetAsync(b->sft.p, 0, I * b->n_sft * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->rtd.p, 0, I * b->n_rtd * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->rz.p, 0, I * b->n_rz * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->vox.p, 0, I * std::max<size_t>(b->n_vox, 1) * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->rbins.p, 0, I * std::max<size_t>(b->n_rbins, 1) * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->region.p, 0, I * lp::kBatchMedia * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->det.p, 0, I * std::max<size_t>(b->n_det, 1) * 2 * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->counters.p, 0, I * LP_NCOUNTERS * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->grad.p, 0, I * grad_stride(b) * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->claimed.p, 0, I * 8, s));
+    LP_BCUDA(b, cudaMemsetAsync(b->frontier.p, 0, 4, s));
+    return LP_OK;
+}
+
+// Grid of the persistent launch: SMs x resident blocks of `config` (queried outside
+// stream capture).
+int prepare_grid(lp_batch *b, int config)
+{
+    int per_sm = 0;
+    LP_BCUDA(b, lp::batch_occupancy(config, b->grad_on, &per_sm));
+    if (per_sm < 1) return bfail(b, LP_ERR_CUDA, "batch configuration %d does not fit on an SM", config);
+    b->grid = b->num_sms * per_sm;
+    return LP_OK;
+}
+
+int enqueue_launch(lp_batch *b, int config)
+{
+    lp::BatchParams B;
+    B.inst = b->params.p;
+    B.claimed = b->claimed.p;
+    B.frontier = b->frontier.p;
+    B.n_inst = (int32_t)b->inst.size();
+    LP_BCUDA(b, lp::launch_batch(config, b->grad_on, B, b->grid, b->stream));
+    return LP_OK;
+}
+
+bool config_eligible(const lp_batch *b, int config)
+{
+    int block, minb, stack;
+    if (lp::batch_config_info(config, &block, &minb, &stack)) return false;
+    for (const lp_ctx *c : b->ctx)
+        if (c->bvh.depth >= stack) return false;
+    return true;
+}
+
+int64_t total_photons(const std::vector<lp_instance> &v)
+{
+    int64_t t = 0;
+    for (const lp_instance &i : v) t += i.n_photons;
+    return t;
+}
+
+// One direct (ungraphed) launch of `config`; device milliseconds of the kernel.
+int timed_launch(lp_batch *b, int config, float *ms)
+{
+    int r = prepare_grid(b, config);
+    if (r) return r;
+    if ((r = enqueue_zero(b))) return r;
+    LP_BCUDA(b, cudaEventRecord(b->ev0, b->stream));
+    if ((r = enqueue_launch(b, config))) return r;
+    LP_BCUDA(b, cudaEventRecord(b->ev1, b->stream));
+    LP_BCUDA(b, cudaEventSynchronize(b->ev1));
+    LP_BCUDA(b, cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return LP_OK;
+}
+
+int copy_counts(lp_batch *b)
+{
+    const size_t I = b->inst.size();
+    b->h_det.resize(I * std::max<size_t>(b->n_det, 1) * 2);
+    b->h_cnt.resize(I * LP_NCOUNTERS);
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_det.data(), b->det.p, b->h_det.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_cnt.data(), b->counters.p, b->h_cnt.size() * 8, cudaMemcpyDeviceToHost,
+                                b->stream));
+    LP_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return LP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lp_batch_config_count(void) { return lp::batch_config_count(); }
+
+int lp_batch_config_info(int32_t config, int32_t *block, int32_t *min_blocks, int32_t *stack)
+{
+    int a, m, s;
+    if (!block || !min_blocks || !stack || lp::batch_config_info(config, &a, &m, &s))
+        return fail(nullptr, LP_ERR_INVALID, "lp_batch_config_info: configuration %d", config);
+    *block = a;
+    *min_blocks = m;
+    *stack = s;
+    return LP_OK;
+}
+
+const char *lp_batch_last_error(const lp_batch *b)
+{
+    if (b) return b->err.c_str();
+    return g_thread_error.c_str();
+}
+
+int lp_batch_create(lp_batch **out, int32_t n_ctx, lp_ctx *const *ctxs)
+{
+    if (!out || n_ctx < 1 || !ctxs) return fail(nullptr, LP_ERR_INVALID, "lp_batch_create: no contexts");
+    *out = nullptr;
+    for (int i = 0; i < n_ctx; ++i)
+        if (!ctxs[i]) return fail(nullptr, LP_ERR_INVALID, "lp_batch_create: context %d is NULL", i);
+    const lp_ctx *c0 = ctxs[0];
+    for (int i = 0; i < n_ctx; ++i) {
+        lp_ctx *c = ctxs[i];
+        if (c->device != c0->device) return fail(nullptr, LP_ERR_INVALID, "lp_batch_create: contexts on two devices");
+        int r = upload(c);
+        if (r) return fail(nullptr, r, "lp_batch_create: context %d: %s", i, c->err.c_str());
+        const lp_geometry &g = c->geo, &g0 = c0->geo;
+        if (std::memcmp(&g, &g0, sizeof g) != 0 || c->n_rbins != c0->n_rbins || c->det_r != c0->det_r ||
+            std::memcmp(c->vox_n, c0->vox_n, sizeof c->vox_n) != 0)
+            return fail(nullptr, LP_ERR_INVALID, "lp_batch_create: context %d has another tally layout", i);
+    }
+    lp_batch *b = new lp_batch;
+    b->device = c0->device;
+    b->num_sms = c0->num_sms;
+    b->ctx.assign(ctxs, ctxs + n_ctx);
+    const lp_geometry &g = c0->geo;
+    b->n_sft = (size_t)g.sft_nx * g.sft_ny * 3;
+    b->n_rtd = (size_t)g.dimR * g.dimAlpha * 3;
+    b->n_rz = (size_t)g.rz_nr * g.rz_nz * 2;
+    b->n_vox = (size_t)n_vox(c0);
+    b->n_rbins = (size_t)c0->n_rbins * 2;
+    b->n_det = c0->det_r.size() / 2;
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+    if (e == cudaSuccess) e = b->frontier.ensure(1);
+    if (e != cudaSuccess) {
+        int r = fail(nullptr, LP_ERR_CUDA, "lp_batch_create: %s", cudaGetErrorString(e));
+        lp_batch_destroy(b);
+        return r;
+    }
+    *out = b;
+    return LP_OK;
+}
+
+void lp_batch_destroy(lp_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graph(b);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int lp_batch_set_instances(lp_batch *b, int32_t n_inst, const lp_instance *in)
+{
+    if (!b || n_inst < 0 || (n_inst > 0 && !in)) return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: bad argument");
+    for (int i = 0; i < n_inst; ++i) {
+        const lp_instance &x = in[i];
+        if (x.context < 0 || x.context >= (int)b->ctx.size())
+            return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: context %d", i, x.context);
+        if (x.n_media < 1 || x.n_media > LP_BATCH_MAX_MEDIA)
+            return bfail(b, LP_ERR_RANGE, "lp_batch_set_instances: instance %d: %d regions (1..%d)", i, x.n_media,
+                         LP_BATCH_MAX_MEDIA);
+        if (b->ctx[x.context]->max_region >= x.n_media)
+            return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: mesh uses region %d", i,
+                         b->ctx[x.context]->max_region);
+        if (x.n_photons < 0 || x.first < 0)
+            return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: negative photon range", i);
+        for (int k = 0; k < 4 * x.n_media; ++k)
+            if (!std::isfinite(x.nmuasg[k]))
+                return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: non-finite media", i);
+    }
+    LP_BCUDA(b, cudaSetDevice(b->device));
+    const size_t I = (size_t)n_inst;
+    if (I != b->inst.size() || !b->params.p) {
+        drop_graph(b);
+        const size_t J = std::max<size_t>(I, 1);
+        LP_BCUDA(b, b->sft.ensure(J * b->n_sft));
+        LP_BCUDA(b, b->rtd.ensure(J * b->n_rtd));
+        LP_BCUDA(b, b->rz.ensure(J * b->n_rz));
+        LP_BCUDA(b, b->vox.ensure(J * std::max<size_t>(b->n_vox, 1)));
+        LP_BCUDA(b, b->rbins.ensure(J * std::max<size_t>(b->n_rbins, 1)));
+        LP_BCUDA(b, b->region.ensure(J * lp::kBatchMedia));
+        LP_BCUDA(b, b->det.ensure(J * std::max<size_t>(b->n_det, 1) * 2));
+        LP_BCUDA(b, b->counters.ensure(J * LP_NCOUNTERS));
+        LP_BCUDA(b, b->grad.ensure(J * grad_stride(b)));
+        LP_BCUDA(b, b->claimed.ensure(J));
+        LP_BCUDA(b, b->media.ensure(J * lp::kBatchMedia));
+        LP_BCUDA(b, b->params.ensure(J));
+    }
+    b->inst.assign(in, in + n_inst);
+    return upload_instances(b);
+}
+
+int lp_batch_set_gradient(lp_batch *b, int enable)
+{
+    if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_set_gradient: batch is NULL");
+    if ((enable != 0) == b->grad_on) return LP_OK;
+    b->grad_on = enable != 0;
+    drop_graph(b);
+    return upload_instances(b);
+}
+
+int lp_batch_set_config(lp_batch *b, int32_t config)
+{
+    if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_set_config: batch is NULL");
+    if (config < -1 || config >= lp::batch_config_count())
+        return bfail(b, LP_ERR_INVALID, "lp_batch_set_config: configuration %d", config);
+    if (config >= 0 && !config_eligible(b, config))
+        return bfail(b, LP_ERR_RANGE, "lp_batch_set_config: configuration %d: traversal stack below BVH depth", config);
+    if (config != b->config) drop_graph(b);
+    b->config = config;
+    return LP_OK;
+}
+
+int lp_batch_autotune(lp_batch *b, int64_t photons, int32_t *best, double *ns_per_photon)
+{
+    if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_autotune: batch is NULL");
+    if (b->inst.empty()) return bfail(b, LP_ERR_STATE, "lp_batch_autotune: no instances");
+    LP_BCUDA(b, cudaSetDevice(b->device));
+    const int K = lp::batch_config_count();
+    const std::vector<lp_instance> saved = b->inst;
+    const int64_t total = std::max<int64_t>(total_photons(saved), 1);
+    const double scale = photons > 0 ? std::min(1.0, (double)photons / (double)total) : 1.0;
+    std::vector<lp_instance> trial = saved;
+    for (lp_instance &x : trial)
+        if (x.n_photons > 0) x.n_photons = std::max<int64_t>(std::min<int64_t>(x.n_photons, 32), (int64_t)(x.n_photons * scale));
+    int r = lp_batch_set_instances(b, (int32_t)trial.size(), trial.data());
+    if (r) return r;
+    const double n_trial = (double)std::max<int64_t>(total_photons(trial), 1);
+    int chosen = -1;
+    double best_ns = 0.0;
+    bool warmed = false;
+    for (int k = 0; k < K; ++k) {
+        double ns = -1.0;
+        if (config_eligible(b, k)) {
+            float ms = 0.0f;
+            if (!warmed) {   // first launch of the process pays for module loading
+                if ((r = timed_launch(b, k, &ms))) return r;
+                warmed = true;
+            }
+            if ((r = timed_launch(b, k, &ms))) return r;
+            ns = (double)ms * 1e6 / n_trial;
+            if (chosen < 0 || ns < best_ns) {
+                chosen = k;
+                best_ns = ns;
+            }
+        }
+        if (ns_per_photon) ns_per_photon[k] = ns;
+    }
+    if ((r = lp_batch_set_instances(b, (int32_t)saved.size(), saved.data()))) return r;
+    if (chosen < 0) return bfail(b, LP_ERR_RANGE, "lp_batch_autotune: no configuration fits these meshes");
+    drop_graph(b);
+    b->config = chosen;
+    if (best) *best = chosen;
+    return LP_OK;
+}
+
+int lp_batch_run(lp_batch *b)
+{
+    if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_run: batch is NULL");
+    if (b->inst.empty()) return LP_OK;
+    LP_BCUDA(b, cudaSetDevice(b->device));
+    int r;
+    if (b->config < 0) {
+        int32_t best;
+        if ((r = lp_batch_autotune(b, 4000000, &best, nullptr))) return r;
+    }
+    if (!b->exec) {
+        // one graph: zero every instance's tallies and counters, then the persistent launch
+        if ((r = prepare_grid(b, b->config))) return r;
+        LP_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        r = enqueue_zero(b);
+        if (!r) r = enqueue_launch(b, b->config);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return bfail(b, LP_ERR_CUDA, "lp_batch_run: capture: %s", cudaGetErrorString(e));
+        b->graph = g;
+        LP_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    LP_BCUDA(b, cudaEventRecord(b->ev0, b->stream));
+    LP_BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
+    LP_BCUDA(b, cudaEventRecord(b->ev1, b->stream));
+    LP_BCUDA(b, cudaEventSynchronize(b->ev1));
+    LP_BCUDA(b, cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    return LP_OK;
+}
+
+int lp_batch_last_ms(const lp_batch *b, float *ms)
+{
+    if (!b || !ms) return fail(nullptr, LP_ERR_INVALID, "lp_batch_last_ms: NULL argument");
+    *ms = b->last_ms;
+    return LP_OK;
+}
+
+int lp_batch_ring_signals(lp_batch *b, double *signal, double *rel_err)
+{
+    if (!b || !signal) return fail(nullptr, LP_ERR_INVALID, "lp_batch_ring_signals: NULL argument");
+    int r = copy_counts(b);
+    if (r) return r;
+    const size_t D = b->n_det, DD = std::max<size_t>(D, 1);
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        const double N = (double)b->h_cnt[i * LP_NCOUNTERS + LP_C_PHOTONS];
+        for (size_t d = 0; d < D; ++d) {
+            const double s1 = (double)b->h_det[(i * DD + d) * 2] / LP_FIX_ONE;
+            const double s2 = (double)b->h_det[(i * DD + d) * 2 + 1] / LP_FIX_ONE;
+            const double m = N > 0 ? s1 / N : 0.0;
+            signal[i * D + d] = m;
+            if (rel_err) {
+                const double se = N > 1 ? std::sqrt(std::max(s2 / N - m * m, 0.0) / N) : 0.0;
+                rel_err[i * D + d] = m > 0 ? se / m : INFINITY;
+            }
+        }
+    }
+    return LP_OK;
+}
+
+int lp_batch_get_tallies(lp_batch *b, int32_t i, lp_tallies *out)
+{
+    if (!b || !out) return fail(nullptr, LP_ERR_INVALID, "lp_batch_get_tallies: NULL argument");
+    if (i < 0 || i >= (int32_t)b->inst.size()) return bfail(b, LP_ERR_INVALID, "lp_batch_get_tallies: instance %d", i);
+    LP_BCUDA(b, cudaSetDevice(b->device));
+    cudaStream_t s = b->stream;
+    const size_t DD = std::max<size_t>(b->n_det, 1);
+    b->h_sft.resize(b->n_sft);
+    b->h_rtd.resize(b->n_rtd);
+    b->h_rz.resize(b->n_rz);
+    b->h_vox.resize(b->n_vox);
+    b->h_rbins.resize(b->n_rbins);
+    b->h_region.resize(lp::kBatchMedia);
+    b->h_det.resize(DD * 2);
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_sft.data(), b->sft.p + i * b->n_sft, b->n_sft * 8, cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_rtd.data(), b->rtd.p + i * b->n_rtd, b->n_rtd * 8, cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_rz.data(), b->rz.p + i * b->n_rz, b->n_rz * 8, cudaMemcpyDeviceToHost, s));
+    if (b->n_vox)
+        LP_BCUDA(b, cudaMemcpyAsync(b->h_vox.data(), b->vox.p + i * b->n_vox, b->n_vox * 8, cudaMemcpyDeviceToHost, s));
+    if (b->n_rbins)
+        LP_BCUDA(b, cudaMemcpyAsync(b->h_rbins.data(), b->rbins.p + i * b->n_rbins, b->n_rbins * 8,
+                                    cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_region.data(), b->region.p + (size_t)i * lp::kBatchMedia, lp::kBatchMedia * 8,
+                                cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_det.data(), b->det.p + i * DD * 2, DD * 2 * 8, cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(out->counters, b->counters.p + (size_t)i * LP_NCOUNTERS, LP_NCOUNTERS * 8,
+                                cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaStreamSynchronize(s));
+    out->sft = b->h_sft.data();
+    out->rtd = b->h_rtd.data();
+    out->rz = b->h_rz.data();
+    out->vox = b->h_vox.data();
+    out->rbins = b->h_rbins.data();
+    out->region = b->h_region.data();
+    out->det = b->h_det.data();
+    out->n_vox = (int64_t)b->n_vox;
+    out->n_rbins = (int64_t)b->n_rbins / 2;
+    out->n_region = b->inst[i].n_media;
+    out->n_det = (int64_t)b->n_det;
+    return LP_OK;
+}
+
+int lp_batch_get_gradient(lp_batch *b, int32_t i, lp_gradient *out)
+{
+    if (!b || !out) return fail(nullptr, LP_ERR_INVALID, "lp_batch_get_gradient: NULL argument");
+    if (i < 0 || i >= (int32_t)b->inst.size()) return bfail(b, LP_ERR_INVALID, "lp_batch_get_gradient: instance %d", i);
+    if (!b->grad_on) return bfail(b, LP_ERR_STATE, "lp_batch_get_gradient: differentiation is off");
+    LP_BCUDA(b, cudaSetDevice(b->device));
+    const lp_instance &in = b->inst[i];
+    const int D = (int)b->n_det, R = in.n_media;
+    const size_t DD = std::max<size_t>(b->n_det, 1);
+    std::vector<uint64_t> det(DD * 2), cnt(LP_NCOUNTERS);
+    b->h_grad.assign(grad_stride(b), 0.0);
+    cudaStream_t s = b->stream;
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_grad.data(), b->grad.p + i * grad_stride(b), grad_stride(b) * 8,
+                                cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(det.data(), b->det.p + i * DD * 2, DD * 2 * 8, cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(cnt.data(), b->counters.p + (size_t)i * LP_NCOUNTERS, LP_NCOUNTERS * 8,
+                                cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaStreamSynchronize(s));
+    form_gradient(det.data(), b->h_grad.data(), (double)cnt[LP_C_PHOTONS], (double)b->ctx[in.context]->factor,
+                  in.nmuasg, D, R, b->gout);
+    fill_gradient(b->gout, D, R, (int64_t)cnt[LP_C_PHOTONS], out);
     return LP_OK;
 }
 

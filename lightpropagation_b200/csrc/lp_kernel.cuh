@@ -87,6 +87,15 @@ struct KParams {
     unsigned long long *work;
 };
 
+// A batch: many instances (one KParams each) traced by one persistent launch.
+constexpr int kBatchMedia = kGradRegions;   // regions per instance in a batch
+struct BatchParams {
+    const KParams *inst;             // [n_inst] per-instance parameters (device memory)
+    unsigned long long *claimed;     // [n_inst] photon indices handed out so far
+    int32_t *frontier;               // lowest instance that may still have unclaimed photons
+    int32_t n_inst;
+};
+
 constexpr uint32_t kCellEmpty = 0x80000000u;
 constexpr uint32_t kCellDense = 127u;
 constexpr int kLocalMaxCells = 8;   // larger segment boxes go to the BVH
@@ -236,6 +245,8 @@ __device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, i
     }
 }
 
+// STACK: traversal stack entries; the host only runs a tree whose depth is below it.
+template <int STACK = kStackDepth>
 __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
                                              float &t_out)
 {
@@ -245,7 +256,7 @@ __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int 
     const float iy = 1.0f / (fabsf(v.y) > 1e-30f ? v.y : copysignf(1e-30f, v.y));
     const float iz = 1.0f / (fabsf(v.z) > 1e-30f ? v.z : copysignf(1e-30f, v.z));
     const float ox = p.x * ix, oy = p.y * iy, oz = p.z * iz;
-    int stack[kStackDepth];
+    int stack[STACK];
     int sp = 0;
     int node = 0;
     for (;;) {
@@ -286,7 +297,7 @@ __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int 
         }
         if (h0 && h1) {
             const bool first0 = tn0 <= tn1;
-            if (sp < kStackDepth) stack[sp++] = first0 ? d.y : d.x;
+            if (sp < STACK) stack[sp++] = first0 ? d.y : d.x;
             node = first0 ? d.x : d.y;
         } else if (h0) {
             node = d.x;
@@ -311,11 +322,12 @@ __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int 
 // accept within the bound, and the result (nearest t, then lowest original index) is
 // the BVH's bit for bit.  Boxes of more than kLocalMaxCells cells, or a dense cell, go
 // to query_nearest; *used_bvh reports which path answered.
+template <int STACK = kStackDepth>
 __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri,
                                           float bound, float &t_out, bool &used_bvh)
 {
     used_bvh = true;
-    if (!P.cell_refs || !(bound < kNoHit)) return query_nearest(M, p, v, ref_tri, bound, t_out);
+    if (!P.cell_refs || !(bound < kNoHit)) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
     const float e = P.g_eps;
     const float qx = p.x + bound * v.x, qy = p.y + bound * v.y, qz = p.z + bound * v.z;
     const int nx = P.g_nx, ny = P.g_ny, nz = P.g_nz;
@@ -326,7 +338,7 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
     const int z0 = min(max((int)floorf((fminf(p.z, qz) - e - P.g_oz) * P.g_inv_h), 0), nz - 1);
     const int z1 = min(max((int)floorf((fmaxf(p.z, qz) + e - P.g_oz) * P.g_inv_h), 0), nz - 1);
     if ((x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1) > kLocalMaxCells)
-        return query_nearest(M, p, v, ref_tri, bound, t_out);
+        return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
     float best = bound;
     int bid = 0x7fffffff;
     for (int z = z0; z <= z1; ++z)
@@ -335,7 +347,7 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
                 const uint32_t w = __ldg(P.cell_word + ((int64_t)z * ny + y) * nx + x);
                 if (w & kCellEmpty) continue;
                 const uint32_t cnt = (w >> 24) & 127u;
-                if (cnt == kCellDense) return query_nearest(M, p, v, ref_tri, bound, t_out);
+                if (cnt == kCellDense) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
                 const int32_t *r = P.cell_refs + (w & 0xffffffu);
                 for (uint32_t k = 0; k < cnt; ++k) test_tri(M, __ldg(r + k), p, v, ref_tri, best, bid);
             }

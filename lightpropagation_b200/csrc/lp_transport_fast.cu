@@ -1,5 +1,6 @@
 // lp_transport_fast.cu -- production instantiation of the transport kernel
-// (Exact = false, compiled with FMA contraction; see lp_transport_impl.cuh).
+// (Exact = false; every unit is built with --fmad=false, the production arithmetic
+// writes its fused multiply-adds explicitly; see lp_transport_impl.cuh).
 #include "lp_transport_impl.cuh"
 
 namespace lp {

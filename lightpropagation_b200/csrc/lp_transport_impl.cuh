@@ -24,7 +24,9 @@
 //               Henyey-Greenstein sampling with precomputed factors, the direction-
 //               cosine update of Wang et al. (MCML, 1995) instead of two Rodrigues
 //               rotations (same distribution: polar angle from HG, uniform azimuth),
-//               vector refraction/reflection, reciprocal multiplies, FMA contraction.
+//               vector refraction/reflection, reciprocal multiplies, explicit fused
+//               multiply-adds.  No unit lets the compiler contract on its own, so a
+//               device function gives the same bits in every kernel that inlines it.
 #pragma once
 #include <algorithm>
 
@@ -73,10 +75,10 @@ __device__ __forceinline__ float hg_cos_theta(const Medium &m, float xi)
         else cosTheta = 2.0f * xi - 1.0f;
     } else {
         if (m.g != 0.0f) {
-            const float g1 = __fdividef(m.hg_a, m.hg_b + m.hg_c * xi);
-            cosTheta = (m.hg_d - g1 * g1) * m.hg_inv2g;
+            const float g1 = __fdividef(m.hg_a, __fmaf_rn(m.hg_c, xi, m.hg_b));
+            cosTheta = __fmaf_rn(-g1, g1, m.hg_d) * m.hg_inv2g;
         } else {
-            cosTheta = 2.0f * xi - 1.0f;
+            cosTheta = __fmaf_rn(2.0f, xi, -1.0f);
         }
     }
     return fminf(fmaxf(cosTheta, -1.0f), 1.0f);
@@ -93,7 +95,7 @@ __device__ __forceinline__ V3 rotate(V3 vec, V3 axis, float c, float s)
 
 __device__ __forceinline__ V3 fast_norm(V3 v)
 {
-    const float r = rsqrtf(dot3(v, v));
+    const float r = rsqrtf(__fmaf_rn(v.x, v.x, __fmaf_rn(v.y, v.y, v.z * v.z)));
     return v3(v.x * r, v.y * r, v.z * r);
 }
 
@@ -125,20 +127,20 @@ __device__ __forceinline__ V3 scatter_direction(V3 v, const Medium &m, float xt,
         // direction-cosine update (Wang, Jacques & Zheng, MCML 1995).  1 - uz^2 is taken
         // as ux^2 + uy^2 (|v| = 1), which keeps its precision near the z axis where the
         // difference form cancels; the axial case scatters about z with uz' = sign(uz) cos.
-        const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+        const float sinTheta = sqrtf(fmaxf(0.0f, __fmaf_rn(-cosTheta, cosTheta, 1.0f)));
         float sinPsi, cosPsi;
         sincospif(2.0f * xp, &sinPsi, &cosPsi);
         V3 r;
-        const float uz2 = v.x * v.x + v.y * v.y;
+        const float uz2 = __fmaf_rn(v.x, v.x, v.y * v.y);
         if (uz2 < 1e-20f) {
             r = v3(sinTheta * cosPsi, sinTheta * sinPsi, v.z > 0.0f ? cosTheta : -cosTheta);
         } else {
             const float it = rsqrtf(uz2);
             const float temp = uz2 * it;  // sqrt(1 - uz^2)
             const float st = sinTheta * it;
-            r = v3(st * (v.x * v.z * cosPsi - v.y * sinPsi) + v.x * cosTheta,
-                   st * (v.y * v.z * cosPsi + v.x * sinPsi) + v.y * cosTheta,
-                   -sinTheta * cosPsi * temp + v.z * cosTheta);
+            r = v3(__fmaf_rn(st, __fmaf_rn(v.x * v.z, cosPsi, -v.y * sinPsi), v.x * cosTheta),
+                   __fmaf_rn(st, __fmaf_rn(v.y * v.z, cosPsi, v.x * sinPsi), v.y * cosTheta),
+                   __fmaf_rn(-sinTheta * cosPsi, temp, v.z * cosTheta));
         }
         return fast_norm(r);
     }
@@ -297,7 +299,7 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
 }
 
 // One iteration of the reference's do-while loop.  Returns false when the photon ends.
-template <bool Exact, bool Grad>
+template <bool Exact, bool Grad, int STACK = kStackDepth>
 __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
                                             unsigned long long *s_region, unsigned long long *s_cnt,
                                             Photon &ph, Counters &cnt, GradAcc *ga)
@@ -319,7 +321,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     int tri;
     const V3 p = v3(ph.px, ph.py, ph.pz), v = v3(ph.vx, ph.vy, ph.vz);
     if (m.ambient) {
-        tri = query_nearest(M, p, v, ph.refTri, kNoHit, thit);
+        tri = query_nearest<STACK>(M, p, v, ph.refTri, kNoHit, thit);
         cnt.query++;
         cnt.bvh++;
     } else if (step < safe_distance(P, cell_at(P, p.x, p.y, p.z))) {
@@ -329,7 +331,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         cnt.skip++;
     } else {
         bool used_bvh;
-        tri = cell_query(P, M, p, v, ph.refTri, step, thit, used_bvh);
+        tri = cell_query<STACK>(P, M, p, v, ph.refTri, step, thit, used_bvh);
         cnt.query++;
         cnt.bvh += used_bvh ? 1u : 0u;
     }

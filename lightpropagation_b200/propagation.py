@@ -39,6 +39,38 @@ def _i32(a):
     return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
 
 
+def tallies_dict(T: N.Tallies, g: N.Geometry) -> dict:
+    """Copy an lp_tallies into numpy arrays shaped like the reference's images."""
+
+    def arr(p, n, shape):
+        if n == 0:
+            return np.zeros(shape, np.uint64)
+        return np.ctypeslib.as_array(p, shape=(n,)).copy().reshape(shape)
+
+    return {
+        "sft": arr(T.sft, g.sft_nx * g.sft_ny * 3, (g.sft_ny, g.sft_nx, 3)),
+        "rtd": arr(T.rtd, g.dimR * g.dimAlpha * 3, (g.dimAlpha, g.dimR, 3)),
+        "rz": arr(T.rz, g.rz_nr * g.rz_nz * 2, (g.rz_nz, g.rz_nr, 2)),
+        "vox": arr(T.vox, T.n_vox, (T.n_vox,)),
+        "rbins": arr(T.rbins, T.n_rbins * 2, (T.n_rbins, 2)),
+        "region": arr(T.region, T.n_region, (T.n_region,)),
+        "det": arr(T.det, T.n_det * 2, (T.n_det, 2)),
+        "counters": {k: int(T.counters[i]) for i, k in enumerate(N.COUNTER_NAMES)},
+    }
+
+
+def gradient_dict(g: N.Gradient) -> dict:
+    D, R = g.n_det, g.n_media
+
+    def arr(p, shape):
+        n = int(np.prod(shape))
+        return np.ctypeslib.as_array(p, shape=(n,)).copy().reshape(shape) if n else np.zeros(shape)
+
+    return {"n_photons": int(g.n_photons), "signal": arr(g.signal, (D,)), "signal_se": arr(g.signal_se, (D,)),
+            "d_mua": arr(g.d_mua, (D, R)), "d_mus": arr(g.d_mus, (D, R)),
+            "d_mua_se": arr(g.d_mua_se, (D, R)), "d_mus_se": arr(g.d_mus_se, (D, R))}
+
+
 class Simulation:
     """One transport context on one GPU."""
 
@@ -125,15 +157,7 @@ class Simulation:
         """Ring signals S_d and dS_d/dmua_r, dS_d/dmus_r with standard errors."""
         g = N.Gradient()
         self._ck(self._L.lp_get_gradient(self._h, C.byref(g)))
-        D, R = g.n_det, g.n_media
-
-        def arr(p, shape):
-            n = int(np.prod(shape))
-            return np.ctypeslib.as_array(p, shape=(n,)).copy().reshape(shape) if n else np.zeros(shape)
-
-        return {"n_photons": int(g.n_photons), "signal": arr(g.signal, (D,)), "signal_se": arr(g.signal_se, (D,)),
-                "d_mua": arr(g.d_mua, (D, R)), "d_mus": arr(g.d_mus, (D, R)),
-                "d_mua_se": arr(g.d_mua_se, (D, R)), "d_mus_se": arr(g.d_mus_se, (D, R))}
+        return gradient_dict(g)
 
     def forward(self, n: int, first: int = 0) -> np.ndarray:
         """Zero the tallies, trace photons [first, first + n) with differentiation on and
@@ -195,23 +219,7 @@ class Simulation:
         g = self.geometry()
         T = N.Tallies()
         self._ck(self._L.lp_get_tallies(self._h, C.byref(T)))
-
-        def arr(p, n, shape):
-            if n == 0:
-                return np.zeros(shape, np.uint64)
-            return np.ctypeslib.as_array(p, shape=(n,)).copy().reshape(shape)
-
-        out = {
-            "sft": arr(T.sft, g.sft_nx * g.sft_ny * 3, (g.sft_ny, g.sft_nx, 3)),
-            "rtd": arr(T.rtd, g.dimR * g.dimAlpha * 3, (g.dimAlpha, g.dimR, 3)),
-            "rz": arr(T.rz, g.rz_nr * g.rz_nz * 2, (g.rz_nz, g.rz_nr, 2)),
-            "vox": arr(T.vox, T.n_vox, (T.n_vox,)),
-            "rbins": arr(T.rbins, T.n_rbins * 2, (T.n_rbins, 2)),
-            "region": arr(T.region, T.n_region, (T.n_region,)),
-            "det": arr(T.det, T.n_det * 2, (T.n_det, 2)),
-            "counters": {k: int(T.counters[i]) for i, k in enumerate(N.COUNTER_NAMES)},
-        }
-        return out
+        return tallies_dict(T, g)
 
     def stats(self) -> dict:
         st = N.Stats()

@@ -119,18 +119,23 @@ ABDOMEN_MEDIA = {
 RING_SEPARATIONS_MM = (20.0, 36.0, 52.0, 68.0, 84.0, 100.0)
 
 
-def curved_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int = 45) -> Workload:
+def curved_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int = 45, head_depth: float = 40.0,
+                   fat=(8.0, 15.0)) -> Workload:
     """Curved mesh abdomen: maternal ellipsoid (semi-axes 150/120/100 mm) with nested
     skin (2 mm), fat (8-15 mm, seeded smooth noise), uterus (10 mm) shells, amniotic
     fluid inside, and a fetal head sphere (radius 45 mm, nearest surface 40 mm below the
     skin); 5 x 20 * freq^2 triangles (202,500 at freq 45).  A 0.4 mm NA-0.22 fibre at the
-    -z pole points into the body; six 1 mm wide ring detectors at 20-100 mm."""
-    tri, nrm, med = meshes.curved_abdomen(freq=freq)
+    -z pole points into the body; six 1 mm wide ring detectors at 20-100 mm.
+    head_depth and fat give the variants of the batched workload; the source, tally
+    layout and outer surface stay the same."""
+    tri, nrm, med = meshes.curved_abdomen(freq=freq, head_depth=head_depth, fat=tuple(fat))
     nmuasg = np.array(ABDOMEN_MEDIA[int(wavelength)], F)
     p0, v0, ep = pencil_source(poi=(0.0, 0.0, -100.0), heading=(0.0, 0.0, 1.0), distance=1.0)
     det_r = np.array([[r - 0.5, r + 0.5] for r in RING_SEPARATIONS_MM], F)
     return Workload(
-        name=f"curved_abdomen_{wavelength}nm_{tri.shape[0]}tri", tri=tri, nrm=nrm, med=med, nmuasg=nmuasg,
+        name=f"curved_abdomen_{wavelength}nm_{tri.shape[0]}tri" +
+             ("" if (head_depth, tuple(fat)) == (40.0, (8.0, 15.0)) else f"_head{head_depth:g}_fat{fat[0]:g}-{fat[1]:g}"),
+        tri=tri, nrm=nrm, med=med, nmuasg=nmuasg,
         p_start=p0, v_start=v0, ep0xyz=ep,
         dimensions=np.array([300.0, 240.0, 200.0], F),
         det_grid=np.array([1.0, 1.0, 1.0, 0.5, 1.0, 1.0], F),
