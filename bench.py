@@ -294,6 +294,68 @@ def traffic_of(workload):
     return (float(b.group(1)) if b else None), (int(float(p.group(1))) if p else None)
 
 
+def batched_section(args, local):
+    """Plain vs batched forms on the batched abdomen workload: the curved-abdomen mesh plus
+    8 variants (fetal-head depth, fat thickness), `--batch-instances` optical-property
+    instances at 660/940 nm with log-uniform budgets in [--batch-min, --batch-max].
+    plain  = one lp_run per instance on its mesh's context (device time of the launches);
+    batched = one lp_batch_run (graph: zero all tallies + one persistent launch).
+    Both trace the same photons and give bit-identical tallies, so the detector errors are
+    matched by construction."""
+    from lightpropagation_b200 import Batch, Instance, Simulation, workloads
+    spec = workloads.batched_abdomen(n_instances=args.batch_instances, budget=(args.batch_min, args.batch_max))
+    sims = [m.apply(Simulation(local), seed=0x4C50) for m in spec.meshes]
+    insts = [Instance(context=x["mesh"], nmuasg=x["nmuasg"], n_photons=x["n_photons"], first=x["first"])
+             for x in spec.instances]
+    total = sum(x.n_photons for x in insts)
+    # plain form
+    plain_ms, plain_det = 0.0, []
+    for x in insts[:2]:                      # warm-up of every context's first launch
+        sims[x.context].set_media(x.nmuasg)
+        sims[x.context].run(1000, 0)
+    t0 = time.perf_counter()
+    for x in insts:
+        s = sims[x.context]
+        s.set_media(x.nmuasg)
+        s.zero()
+        s.run(x.n_photons, x.first)
+        plain_ms += s.kernel_ms()
+        plain_det.append(s.tallies()["det"] if len(plain_det) < 4 else None)
+    plain_wall = time.perf_counter() - t0
+    # batched form
+    b = Batch(sims)
+    b.set_instances(insts)
+    best, ns = b.autotune(min(total, 8_000_000))
+    b.run()                                  # graph capture + first replay
+    runs = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        b.run()
+        runs.append((b.last_ms(), time.perf_counter() - t0))
+    batch_ms = min(r[0] for r in runs)
+    identical = all(np.array_equal(b.tallies(i)["det"], plain_det[i]) for i in range(min(4, len(insts))))
+    sig, rel = b.ring_signals()
+    from lightpropagation_b200.batch import config_table
+    cfg = config_table()[best]
+    out = {"instances": len(insts), "meshes": len(spec.meshes),
+           "triangles": [int(m.n_tri) for m in spec.meshes], "photons": int(total),
+           "budget_range": [args.batch_min, args.batch_max],
+           "plain_photons_per_s": total / (plain_ms * 1e-3), "plain_wall_photons_per_s": total / plain_wall,
+           "batched_photons_per_s": total / (batch_ms * 1e-3),
+           "batched_wall_photons_per_s": total / min(r[1] for r in runs),
+           "batched_vs_plain": plain_ms / batch_ms,
+           "tallies_identical_to_plain": bool(identical),
+           "instances_at_1pct_rse_ring0": int(np.sum(rel[:, 0] <= 0.01)),
+           "autotuned_config": cfg, "autotune_ns_per_photon": [float(v) for v in ns],
+           "note": ("budgets scaled from the workload's 1e6-1e8 to keep the bench within minutes; "
+                    "plain = device time of one launch per instance, batched = device time of one graph launch "
+                    "including the zeroing of all instance tallies")}
+    b.close()
+    for s in sims:
+        s.close()
+    return out
+
+
 def ours_arm(args, cases):
     import torch
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -457,6 +519,12 @@ def ours_arm(args, cases):
             "peak_source": "FP32 FMA peak measured in-run by lp_fp32_peak (MEASURED_PEAKS.json has no FP32 figure)",
             "events_per_photon": events}
 
+    batched = None
+    if world == 1 and args.batch_instances > 0:
+        sim.close()
+        batched = batched_section(args, local)
+        sim = None
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -482,10 +550,11 @@ def ours_arm(args, cases):
                        "bvh_nodes_in_smem": st["nodes_smem"], "tris_in_smem": st["tris_smem"]},
             "wall_s": wall, "clocks": clk, "gpu_launches": args.steps * ncase,
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "detector_error": rse, "gradient": gradient,
+            "detector_error": rse, "gradient": gradient, "batched": batched,
             "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line))
-    sim.close()
+    if sim is not None:
+        sim.close()
     return 0
 
 
@@ -501,6 +570,10 @@ def main():
                     help="photons per launch per GPU (default: the workload's, 1e7 for the abdomen)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient-cost launches")
+    ap.add_argument("--batch-instances", type=int, default=512, help="instances of the plain-vs-batched "
+                    "comparison (0 skips it)")
+    ap.add_argument("--batch-min", type=float, default=1e4, help="smallest instance photon budget")
+    ap.add_argument("--batch-max", type=float, default=1e6, help="largest instance photon budget")
     args = ap.parse_args()
     cases = load_cases(args.workload, args.photons)
     if args.impl == "reference":

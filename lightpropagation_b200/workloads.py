@@ -147,3 +147,75 @@ def curved_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int
 
 WORKLOADS = {"plain_slab": plain_slab, "curved_abdomen": curved_abdomen,
              "curved_abdomen_940": lambda n_photons=10_000_000: curved_abdomen(n_photons, 940)}
+
+
+# ------------------------------------------------------------------ batched workload
+# Molar extinction coefficients of oxy- and deoxyhaemoglobin [cm^-1 / M] at the two
+# wavelengths, rounded from S. Prahl's public compilation of hemoglobin absorption.
+# Inputs of the synthetic benchmark, not measurements.
+HB_EXTINCTION = {660: (319.6, 3226.56), 940: (1214.0, 693.44)}
+HB_MOLAR = 150.0 / 64500.0            # whole blood: 150 g/L haemoglobin, 64.5 kg/mol
+# per-region background absorption [1/mm] and share of the drawn blood fraction
+BACKGROUND_MUA = {660: [0.0, 0.005, 0.002, 0.005, 0.001, 0.005], 940: [0.0, 0.008, 0.004, 0.008, 0.001, 0.008]}
+BLOOD_SHARE = [0.0, 1.0, 0.5, 1.5, 0.0, 1.0]
+MATERNAL, FETAL = (1, 2, 3), (5,)
+
+
+def blood_mua(spo2: float, wavelength: int) -> float:
+    """Absorption coefficient of whole blood [1/mm] at saturation spo2 (0..1)."""
+    e_ox, e_de = HB_EXTINCTION[int(wavelength)]
+    return float(np.log(10.0) * (spo2 * e_ox + (1.0 - spo2) * e_de) * HB_MOLAR / 10.0)
+
+
+def tissue_table(wavelength: int, spo2_maternal: float, spo2_fetal: float, bf_maternal: float, bf_fetal: float,
+                 mus_scale=None) -> np.ndarray:
+    """(n, mua, mus, g) per abdomen region: mua = background + blood share x blood
+    fraction x blood absorption at the region's saturation; mus = base x mus_scale."""
+    base = np.array(ABDOMEN_MEDIA[int(wavelength)], F)
+    nm = base.copy()
+    for r in range(1, base.shape[0]):
+        mua = BACKGROUND_MUA[int(wavelength)][r]
+        if r in MATERNAL:
+            mua += BLOOD_SHARE[r] * bf_maternal * blood_mua(spo2_maternal, wavelength)
+        elif r in FETAL:
+            mua += BLOOD_SHARE[r] * bf_fetal * blood_mua(spo2_fetal, wavelength)
+        else:
+            mua = base[r, 1]
+        nm[r, 1] = mua
+        if mus_scale is not None and r != 4:
+            nm[r, 2] = base[r, 2] * mus_scale[r]
+    return nm
+
+
+@dataclass
+class BatchSpec:
+    meshes: list                # Workloads (one per mesh; same source and tally layout)
+    instances: list             # dicts: mesh, wavelength, nmuasg, n_photons, first, spo2_m, spo2_f
+
+
+def batched_abdomen(n_instances: int = 512, budget=(1e6, 1e8), n_variants: int = 8, freq: int = 45,
+                    variant_freq: int = 30, seed: int = 3) -> BatchSpec:
+    """The batched forward workload: the curved-abdomen mesh plus n_variants meshes with
+    fetal-head depth U(30, 70) mm and fat thickness in [5, 25] mm (reduced tessellation),
+    and n_instances optical-property draws -- fetal SpO2 U(30, 70) %, maternal SpO2
+    U(90, 100) %, blood fractions U(2, 8) %, mus lognormal (sigma 0.2) around each region's
+    base value -- alternating 660 and 940 nm, with photon budgets log-uniform in
+    `budget`.  Instance i uses mesh i mod (n_variants + 1)."""
+    rng = np.random.default_rng(seed)
+    meshes_ = [curved_abdomen(wavelength=660, freq=freq)]
+    for _ in range(n_variants):
+        depth = float(np.round(rng.uniform(30.0, 70.0), 1))
+        lo = float(np.round(rng.uniform(5.0, 15.0), 1))
+        hi = float(np.round(min(25.0, lo + rng.uniform(5.0, 10.0)), 1))
+        meshes_.append(curved_abdomen(wavelength=660, freq=variant_freq, head_depth=depth, fat=(lo, hi)))
+    out, first = [], 0
+    for i in range(n_instances):
+        wl = 660 if i % 2 == 0 else 940
+        s_f, s_m = rng.uniform(0.30, 0.70), rng.uniform(0.90, 1.00)
+        bf_m, bf_f = rng.uniform(0.02, 0.08), rng.uniform(0.02, 0.08)
+        mus_scale = np.exp(0.2 * rng.standard_normal(6))
+        n = int(np.exp(rng.uniform(np.log(budget[0]), np.log(budget[1]))))
+        out.append({"mesh": i % len(meshes_), "wavelength": wl, "spo2_m": s_m, "spo2_f": s_f,
+                    "nmuasg": tissue_table(wl, s_m, s_f, bf_m, bf_f, mus_scale), "n_photons": n, "first": first})
+        first += n
+    return BatchSpec(meshes_, out)
