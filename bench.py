@@ -513,9 +513,8 @@ def ours_arm(args, cases):
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None,
             "traffic": traffic,
-            "traffic_note": (f"DRAM bytes of one {traffic_photons}-photon launch (ncu, profiles/); the traffic is "
-                             f"the touch of the L2-resident tallies, safety grid and BVH and does not grow "
-                             f"with the photon count") if traffic is not None else None,
+            "traffic_note": (f"dram__bytes_read.sum + dram__bytes_write.sum of one {traffic_photons}-photon 660 nm "
+                             f"launch of this workload (ncu, profiles/)") if traffic is not None else None,
             "peak_source": "FP32 FMA peak measured in-run by lp_fp32_peak (MEASURED_PEAKS.json has no FP32 figure)",
             "events_per_photon": events}
 

@@ -304,6 +304,8 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
                                             unsigned long long *s_region, unsigned long long *s_cnt,
                                             Photon &ph, Counters &cnt, GradAcc *ga)
 {
+    // the cell word is read first so that its load overlaps the Philox rounds
+    const uint32_t word = cell_at(P, ph.px, ph.py, ph.pz);
     EventRng rng;
     rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
     const Medium m = s_media[ph.curr];
@@ -324,7 +326,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         tri = query_nearest<STACK>(M, p, v, ph.refTri, kNoHit, thit);
         cnt.query++;
         cnt.bvh++;
-    } else if (step < safe_distance(P, cell_at(P, p.x, p.y, p.z))) {
+    } else if (step < safe_distance(P, word)) {
         // no triangle within the step: the bounded query would return "no hit"
         tri = -1;
         thit = kNoHit;
