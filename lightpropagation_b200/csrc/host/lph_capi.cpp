@@ -72,6 +72,44 @@ void lph_source(const lph_model *m, float *p_start, float *v_start, float *ep0xy
     std::memcpy(ep0xyz, m->ep0xyz, 48);
 }
 
+// Write one reference-format log (lp::Logs) of an image with extent ext and ncomp
+// components, values ordered x fastest then y (component innermost), as lp::ImageData
+// stores them.  kind: 0 SaveSurfaceArr, 1 SaveRecordRd, 2 CalcReflectancePerRadius,
+// 3 CalcReflectancePerAngle, 4 FluenceZ.  Returns 0, or 1 for an unknown kind.
+int lph_write_log(const char *dir, const char *fname, int kind, const float *values, const int32_t *ext, int ncomp,
+                  const float *grid, int64_t photons)
+{
+    const int e[6] = {ext[0], ext[1], ext[2], ext[3], ext[4], ext[5]};
+    auto img = std::make_shared<lp::ImageData>(e, ncomp);
+    std::memcpy(img->data().data(), values, img->data().size() * sizeof(float));
+    lp::Logs logs;
+    logs.SetSaveDir(dir);
+    logs.SetGridDimensions(std::vector<float>(grid, grid + 6));
+    logs.SetNumberOfPhotons(photons);
+    switch (kind) {
+    case 0: logs.SaveSurfaceArr(fname, img); return 0;
+    case 1: logs.SaveRecordRd(fname, img); return 0;
+    case 2: logs.CalcReflectancePerRadius(fname, img); return 0;
+    case 3: logs.CalcReflectancePerAngle(fname, img); return 0;
+    case 4: logs.FluenceZ(fname, img); return 0;
+    default: return 1;
+    }
+}
+
+// lp::Analysis surface sums of an SFT image (3 components): surf, fetal, trans.
+void lph_surface_sums(const float *values, const int32_t *ext, double *out)
+{
+    const int e[6] = {ext[0], ext[1], ext[2], ext[3], ext[4], ext[5]};
+    auto img = std::make_shared<lp::ImageData>(e, 3);
+    std::memcpy(img->data().data(), values, img->data().size() * sizeof(float));
+    lp::Analysis a;
+    a.SetRTdxyLogs(img);
+    a.CalculateSurfaceSums();
+    out[0] = a.SurfaceSum();
+    out[1] = a.FetalSum();
+    out[2] = a.TransSum();
+}
+
 void lph_grid(const lph_model *m, float *dims, float *det_grid, int32_t *fetal_id, float *chance, float *w_th,
               float *ppu, int64_t *photons)
 {
