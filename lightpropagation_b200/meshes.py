@@ -168,6 +168,100 @@ def curved_abdomen(freq: int = 45, axes=(150.0, 120.0, 100.0), skin=2.0, fat=(8.
     return tri, face_normals(tri), med
 
 
+class GradientNoise:
+    """Seeded 3-D gradient noise after Perlin's improved noise (SIGGRAPH 2002): a lattice
+    with a shuffled permutation table, one of 12 edge gradients per lattice point, the
+    quintic fade 6t^5 - 15t^4 + 10t^3 and trilinear blending.  Values lie in about [-1, 1]."""
+
+    GRAD = np.array([[1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1],
+                     [-1, 0, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1]], np.float64)
+
+    def __init__(self, seed: int):
+        perm = np.random.default_rng(seed).permutation(256)
+        self.p = np.concatenate([perm, perm]).astype(np.int64)
+
+    def __call__(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, np.float64)
+        i0 = np.floor(x).astype(np.int64)
+        f = x - i0
+        i0 &= 255
+        w = f * f * f * (f * (f * 6.0 - 15.0) + 10.0)
+        p = self.p
+        out = 0.0
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    h = p[p[p[i0[:, 0] + dx] + i0[:, 1] + dy] + i0[:, 2] + dz] % 12
+                    g = self.GRAD[h]
+                    d = g[:, 0] * (f[:, 0] - dx) + g[:, 1] * (f[:, 1] - dy) + g[:, 2] * (f[:, 2] - dz)
+                    wx = w[:, 0] if dx else 1.0 - w[:, 0]
+                    wy = w[:, 1] if dy else 1.0 - w[:, 1]
+                    wz = w[:, 2] if dz else 1.0 - w[:, 2]
+                    out = out + wx * wy * wz * d
+        return out
+
+
+def octave_noise(points: np.ndarray, seed: int, octaves: int = 3, scale: float = 40.0) -> np.ndarray:
+    """Sum of `octaves` octaves of gradient noise (frequency x2, amplitude /2 each) at
+    points [N, 3] (mm), with a feature size of `scale` mm, divided by the sum of the
+    octave amplitudes (a fixed field: the value at a point does not depend on the others)."""
+    noise = GradientNoise(seed)
+    s = np.zeros(points.shape[0])
+    amp, tot = 1.0, 0.0
+    for o in range(octaves):
+        s += amp * noise(points * (2.0 ** o) / scale + 17.31 * o)
+        tot += amp
+        amp *= 0.5
+    return np.clip(s / tot, -1.0, 1.0)
+
+
+def deformed_abdomen(freq: int = 129, axes=(150.0, 120.0, 100.0), skin=2.0, fat=(8.0, 15.0), uterus=10.0,
+                     head_radius=45.0, head_depth=40.0, placenta_center=(0.0, 0.0, 52.0),
+                     placenta_axes=(45.0, 45.0, 8.0), amplitude=3.0, seed=5):
+    """The abdomen of `curved_abdomen` with a placenta and seeded 3-octave gradient-noise
+    displacement of every surface (amplitude `amplitude` mm along the surface normal).
+
+    Regions: 0 ambient, 1 skin, 2 fat, 3 uterus, 4 amniotic fluid, 5 fetal head,
+    6 placenta (an ellipsoid in the amniotic fluid on the uterine wall opposite the
+    source).  The four nested shells share one displacement field, so every layer keeps
+    its thickness; the head and placenta get their own fields.  Six geodesic surfaces of
+    20 * freq^2 triangles: freq 129 gives 1,996,920 triangles.  Returns (tri, nrm, med,
+    pole): pole is the displaced outer-surface point on the -z axis (the source site)."""
+    a, b, c = axes
+    u, faces = geodesic_sphere(freq)
+    p0 = u * np.array([a, b, c])[None, :]
+    nrm = p0 / np.array([a * a, b * b, c * c])[None, :]
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    disp = amplitude * octave_noise(p0, seed)
+    t_fat = fat[0] + (fat[1] - fat[0]) * smooth_noise(u, 2)
+    depths = [np.zeros(len(u)), np.full(len(u), skin), skin + t_fat, skin + t_fat + uterus]
+    regions = [(1, 0), (2, 1), (3, 2), (4, 3)]
+    tris, meds = [], []
+    for d, (inner, outer) in zip(depths, regions):
+        pts = p0 + (disp - d)[:, None] * nrm
+        t, m = _shell_triangles(pts, faces, inner, outer)
+        tris.append(t)
+        meds.append(m)
+    centre = np.array([0.0, 0.0, -c + head_depth + head_radius])
+    head = centre[None, :] + (head_radius + amplitude * octave_noise(u * head_radius, seed + 1))[:, None] * u
+    t, m = _shell_triangles(head, faces, 5, 4)
+    tris.append(t)
+    meds.append(m)
+    pc = np.array(placenta_center)[None, :]
+    pl = pc + u * np.array(placenta_axes)[None, :]
+    pn = u / np.array(placenta_axes)[None, :]
+    pn /= np.linalg.norm(pn, axis=1, keepdims=True)
+    pl = pl + (amplitude * octave_noise(pl, seed + 2))[:, None] * pn * 0.5
+    t, m = _shell_triangles(pl, faces, 6, 4)
+    tris.append(t)
+    meds.append(m)
+    tri = np.concatenate(tris)
+    med = np.concatenate(meds)
+    # the outer surface on the -z axis, where the normal is -z
+    pole = np.array([0.0, 0.0, -c - amplitude * octave_noise(np.array([[0.0, 0.0, -c]]), seed)[0]], F)
+    return tri, face_normals(tri), med, pole
+
+
 def write_obj(path, tri: np.ndarray, med: np.ndarray, names) -> None:
     """Write a mesh in the reference's OBJ convention (ImportExport.cpp:952-1053):
     runs of triangles with the same (inner, outer) pair become `o <names[inner]>`,

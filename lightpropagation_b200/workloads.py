@@ -145,8 +145,33 @@ def curved_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int
         fiber_radius=0.2, fiber_na=0.22, compat=0)
 
 
+PLACENTA = [1.4, 0.05, 10.0, 0.9]
+
+
+def deformed_abdomen(n_photons: int = 10_000_000, wavelength: int = 660, freq: int = 129,
+                     amplitude: float = 3.0, seed: int = 5, head_depth: float = 40.0) -> Workload:
+    """The large deformed abdomen: the curved abdomen's shells plus a placenta (mua 0.05,
+    mus 10 /mm), every surface displaced by seeded 3-octave gradient noise of amplitude
+    3 mm; 7 regions and 6 x 20 * freq^2 triangles (1,996,920 at freq 129).  Same fibre
+    source (at the displaced pole), rings and tally layout as curved_abdomen."""
+    tri, nrm, med, pole = meshes.deformed_abdomen(freq=freq, amplitude=amplitude, seed=seed, head_depth=head_depth)
+    nmuasg = np.array(ABDOMEN_MEDIA[int(wavelength)] + [PLACENTA], F)
+    p0, v0, ep = pencil_source(poi=tuple(float(x) for x in pole), heading=(0.0, 0.0, 1.0), distance=1.0)
+    det_r = np.array([[r - 0.5, r + 0.5] for r in RING_SEPARATIONS_MM], F)
+    return Workload(
+        name=f"deformed_abdomen_{wavelength}nm_{tri.shape[0]}tri", tri=tri, nrm=nrm, med=med, nmuasg=nmuasg,
+        p_start=p0, v_start=v0, ep0xyz=ep,
+        dimensions=np.array([300.0, 240.0, 200.0], F),
+        det_grid=np.array([1.0, 1.0, 1.0, 0.5, 1.0, 1.0], F),
+        fetal_id=5, n_photons=n_photons,
+        vox_n=(200, 200, 120), vox_d=(1.0, 1.0, 1.0), n_rbins=300, rbin_dr=0.5, det_r=det_r,
+        region_names=["ambient", "skin", "fat", "uterus", "amniotic", "fetal_head", "placenta"],
+        fiber_radius=0.2, fiber_na=0.22, compat=0)
+
+
 WORKLOADS = {"plain_slab": plain_slab, "curved_abdomen": curved_abdomen,
-             "curved_abdomen_940": lambda n_photons=10_000_000: curved_abdomen(n_photons, 940)}
+             "curved_abdomen_940": lambda n_photons=10_000_000: curved_abdomen(n_photons, 940),
+             "deformed_abdomen": deformed_abdomen}
 
 
 # ------------------------------------------------------------------ batched workload
