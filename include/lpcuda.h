@@ -210,6 +210,10 @@ int lp_batch_ring_signals(lp_batch *b, double *signal, double *rel_err);
 int lp_batch_get_tallies(lp_batch *b, int32_t inst, lp_tallies *out);
 int lp_batch_get_gradient(lp_batch *b, int32_t inst, lp_gradient *out);
 
+/* Shared memory per block (bytes) for BVH nodes and triangles staged by the transport
+ * kernel; what a block does not take stays L1 cache for the cell grid, tallies and the
+ * rest of the mesh.  No reference counterpart; results do not depend on it. */
+int lp_set_smem_budget(lp_ctx *ctx, int32_t bytes);
 /* Whether cells touched by triangles list them (1, default) or hold no information
  * (0: every query that the safety bound does not skip descends the BVH).  Results are
  * identical either way; lp_query_triangles follows the same setting. */

@@ -109,6 +109,7 @@ _SIGS = {
     "lp_set_arithmetic": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_safety_grid": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_set_cell_lists": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_set_smem_budget": ([C.c_void_p, C.c_int32], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "lp_run_async": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),

@@ -172,6 +172,7 @@ struct lp_ctx {
     DevBuf<unsigned long long> sft, rtd, rz, vox, rbins, region, det, counters, work;
     DevBuf<float> exit_rec;
     // safety grid (lp_set_safety_grid)
+    int smem_budget = 64 * 1024;   // shared memory per block for staged BVH nodes and triangles
     int64_t grid_max_cells = int64_t(1) << 24;
     bool grid_dirty = true;
     bool cell_lists = true;
@@ -794,6 +795,15 @@ int lp_set_safety_grid(lp_ctx *c, int64_t max_cells)
     return LP_OK;
 }
 
+int lp_set_smem_budget(lp_ctx *c, int32_t bytes)
+{
+    if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_smem_budget: ctx is NULL");
+    if (bytes < lp::smem_bytes(0, 0) || bytes > 200 * 1024)
+        return fail(c, LP_ERR_RANGE, "lp_set_smem_budget: %d bytes (%d..%d)", bytes, lp::smem_bytes(0, 0), 200 * 1024);
+    c->smem_budget = bytes;
+    return LP_OK;
+}
+
 int lp_set_gradient(lp_ctx *c, int enable)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_gradient: ctx is NULL");
@@ -893,7 +903,7 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
         return fail(c, LP_ERR_RANGE, "lp_run: differentiation supports at most %d regions (%d set)",
                     lp::kGradRegions, c->n_media);
     int nodes_smem, tris_smem;
-    smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
+    smem_plan(c, c->smem_budget, nodes_smem, tris_smem);
     const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     int per_sm = 0;
     if (c->grad_on)
@@ -1098,7 +1108,7 @@ int lp_query_triangles(lp_ctx *c, int64_t n, const float *orig, const float *dir
     LP_CUDA(c, cudaMemcpyAsync(tm.p, t_max, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     LP_CUDA(c, cudaMemcpyAsync(rf.p, ref_tri, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     int nodes_smem, tris_smem;
-    smem_plan(c, 64 * 1024, nodes_smem, tris_smem);
+    smem_plan(c, c->smem_budget, nodes_smem, tris_smem);
     KParams P;
     fill_params(c, P, 0, 0, nodes_smem, tris_smem);
     const int smem = lp::smem_bytes(nodes_smem, tris_smem);

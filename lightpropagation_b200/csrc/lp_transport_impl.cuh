@@ -35,6 +35,11 @@
 namespace lp {
 
 constexpr int kBlock = 256;
+// Resident blocks per SM the single-instance kernel is compiled for (register budget
+// 65536 / (kBlock x this)); the batched kernel's configurations are autotuned instead.
+#ifndef LP_TRANSPORT_MIN_BLOCKS
+#define LP_TRANSPORT_MIN_BLOCKS 3
+#endif
 
 struct Photon {
     float px, py, pz, vx, vy, vz;
@@ -566,7 +571,7 @@ __device__ __forceinline__ MeshView stage_mesh(const KParams &P, unsigned char *
 }
 
 template <bool Exact, bool Grad>
-__global__ void __launch_bounds__(kBlock, 3) transport_kernel(const __grid_constant__ KParams P)
+__global__ void __launch_bounds__(kBlock, LP_TRANSPORT_MIN_BLOCKS) transport_kernel(const __grid_constant__ KParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SmemLayout L = smem_layout(P.nodes_smem, P.tris_smem);

@@ -184,6 +184,10 @@ class Simulation:
         results are unchanged either way)."""
         self._ck(self._L.lp_set_cell_lists(self._h, 1 if enable else 0))
 
+    def set_smem_budget(self, nbytes: int):
+        """Shared memory per block for staged BVH nodes and triangles (the rest is L1)."""
+        self._ck(self._L.lp_set_smem_budget(self._h, int(nbytes)))
+
     def set_max_steps(self, n: int):
         self._ck(self._L.lp_set_max_steps(self._h, int(n)))
 
