@@ -58,12 +58,14 @@ struct DevBuf {
     cudaError_t ensure(size_t count)
     {
         if (count <= n && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
+        release();
         cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        return e;
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        n = count;
+        return cudaSuccess;
     }
     void release()
     {
