@@ -1,10 +1,18 @@
 // lp_bvh.cpp -- binned-SAH BVH build on the host (see lp_bvh.hpp for the layout).
+//
+// The primitives (box, centroid, original index) are stored contiguously and partitioned
+// in place, so every pass over a node reads memory in order.  The nodes above a size
+// threshold are split on the calling thread; the subtrees below them are independent
+// ranges of the primitive array and are built on worker threads, then appended in a
+// fixed order.  The tree is therefore the same for any thread count.
 #include "lp_bvh.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 namespace lp {
 namespace {
@@ -35,6 +43,12 @@ struct Box {
     }
 };
 
+struct Prim {
+    Box box;
+    float c[3];  // centroid of the box
+    int32_t id;  // original triangle index
+};
+
 struct BNode {
     Box box;
     int32_t child[2] = {-1, -1};
@@ -44,116 +58,158 @@ struct BNode {
 
 constexpr int kBins = 32;
 
-}  // namespace
-
-void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
+inline int bin_of(float x, float lo, double sc)
 {
-    out = Bvh();
-    std::vector<Box> tb((size_t)n);
-    std::vector<float> cen((size_t)n * 3);
-    Box scene;
-    double max_abs = 0.0;
-    for (int64_t i = 0; i < n; ++i) {
-        const float *t = tri + 9 * i;
-        for (int v = 0; v < 3; ++v) {
-            tb[i].grow(t + 3 * v);
-            for (int a = 0; a < 3; ++a) max_abs = std::max(max_abs, (double)std::fabs(t[3 * v + a]));
-        }
-        for (int a = 0; a < 3; ++a) cen[3 * i + a] = 0.5f * (tb[i].lo[a] + tb[i].hi[a]);
-        scene.grow(tb[i]);
-    }
-    double ext = 0.0;
-    if (n > 0)
-        for (int a = 0; a < 3; ++a) ext = std::max(ext, (double)scene.hi[a] - scene.lo[a]);
-    const float margin = (float)(1e-5 * std::max(ext, max_abs) + 1e-30);
-    out.margin = margin;
-    for (int a = 0; a < 3; ++a) {
-        out.lo[a] = n ? scene.lo[a] : 0.0f;
-        out.hi[a] = n ? scene.hi[a] : 0.0f;
-    }
+    const int b = (int)((x - lo) * sc);
+    return std::min(std::max(b, 0), kBins - 1);
+}
 
-    std::vector<int64_t> idx((size_t)n);
-    for (int64_t i = 0; i < n; ++i) idx[i] = i;
-    std::vector<BNode> nodes;
-    nodes.reserve((size_t)(2 * n / std::max(1, leaf_target) + 4));
-    nodes.push_back(BNode());
-    nodes[0].first = 0;
-    nodes[0].count = n;
-    std::vector<int32_t> work{0};
-    while (!work.empty()) {
-        int32_t ni = work.back();
-        work.pop_back();
-        BNode nd = nodes[ni];
-        Box cb;  // centroid bounds
-        nd.box = Box();
-        for (int64_t k = nd.first; k < nd.first + nd.count; ++k) {
-            nd.box.grow(tb[idx[k]]);
-            cb.grow(&cen[3 * idx[k]]);
+// Runs fn(k, lo, hi) over nt contiguous chunks of [0, n), chunk 0 on the calling thread.
+template <class Fn>
+void for_chunks(int nt, int64_t n, Fn fn)
+{
+    std::vector<std::thread> pool;
+    for (int k = 1; k < nt; ++k) pool.emplace_back([&, k]() { fn(k, n * k / nt, n * (k + 1) / nt); });
+    fn(0, 0, n / nt);
+    for (std::thread &th : pool) th.join();
+}
+
+constexpr int64_t kParallelNode = 65536;  // nodes at least this large bin on several threads
+
+// Computes the node's box and either marks it a leaf (returns false) or partitions its
+// primitives at the best SAH bin boundary and returns true with `mid` the first index of
+// the right half.  Min/max and integer counts merge exactly, so the chunked binning of
+// large nodes gives the same bins as one pass.
+bool split_node(Prim *pr, BNode &nd, int leaf_target, int64_t &mid, int n_threads)
+{
+    Box cb;  // centroid bounds
+    nd.box = Box();
+    Prim *const p0 = pr + nd.first, *const p1 = pr + nd.first + nd.count;
+    const int nt = nd.count >= kParallelNode ? n_threads : 1;
+    if (nt > 1) {
+        std::vector<Box> part_box((size_t)nt), part_cb((size_t)nt);
+        for_chunks(nt, nd.count, [&](int k, int64_t lo, int64_t hi) {
+            Box b, c;  // local, so that the threads share no cache line while they scan
+            for (const Prim *p = p0 + lo; p < p0 + hi; ++p) {
+                b.grow(p->box);
+                c.grow(p->c);
+            }
+            part_box[k] = b;
+            part_cb[k] = c;
+        });
+        for (int k = 0; k < nt; ++k) {
+            nd.box.grow(part_box[k]);
+            cb.grow(part_cb[k]);
         }
-        bool make_leaf = nd.count <= leaf_target;
-        int best_axis = -1, best_bin = -1;
-        double best_cost = DBL_MAX;
-        if (!make_leaf) {
-            for (int a = 0; a < 3; ++a) {
-                float lo = cb.lo[a], hi = cb.hi[a];
-                if (!(hi > lo)) continue;
-                Box bb[kBins];
-                int64_t bc[kBins] = {0};
-                const double sc = kBins / ((double)hi - lo);
-                for (int64_t k = nd.first; k < nd.first + nd.count; ++k) {
-                    int b = (int)((cen[3 * idx[k] + a] - lo) * sc);
-                    b = std::min(std::max(b, 0), kBins - 1);
-                    bb[b].grow(tb[idx[k]]);
-                    bc[b]++;
+    } else {
+        for (const Prim *p = p0; p < p1; ++p) {
+            nd.box.grow(p->box);
+            cb.grow(p->c);
+        }
+    }
+    bool make_leaf = nd.count <= leaf_target;
+    int best_axis = -1, best_bin = -1;
+    double best_cost = DBL_MAX;
+    if (!make_leaf) {
+        bool live[3];
+        double sc[3];
+        for (int a = 0; a < 3; ++a) {
+            live[a] = cb.hi[a] > cb.lo[a];
+            sc[a] = live[a] ? kBins / ((double)cb.hi[a] - cb.lo[a]) : 0.0;
+        }
+        struct Bins {
+            Box bb[3][kBins];
+            int64_t bc[3][kBins] = {};
+        };
+        auto bin_range = [&](Bins &B, const Prim *q0, const Prim *q1) {
+            for (const Prim *p = q0; p < q1; ++p)
+                for (int a = 0; a < 3; ++a) {
+                    if (!live[a]) continue;
+                    const int b = bin_of(p->c[a], cb.lo[a], sc[a]);
+                    B.bb[a][b].grow(p->box);
+                    B.bc[a][b]++;
                 }
-                double ra[kBins];
-                int64_t rn[kBins];
-                Box acc;
-                int64_t cnt = 0;
-                for (int b = kBins - 1; b > 0; --b) {
-                    acc.grow(bb[b]);
-                    cnt += bc[b];
-                    ra[b] = acc.area();
-                    rn[b] = cnt;
-                }
-                acc = Box();
-                cnt = 0;
-                for (int b = 0; b < kBins - 1; ++b) {
-                    acc.grow(bb[b]);
-                    cnt += bc[b];
-                    if (cnt == 0 || rn[b + 1] == 0) continue;
-                    double c = acc.area() * (double)cnt + ra[b + 1] * (double)rn[b + 1];
-                    if (c < best_cost) {
-                        best_cost = c;
-                        best_axis = a;
-                        best_bin = b;
+        };
+        Bins all;
+        if (nt > 1) {
+            std::vector<Bins> part((size_t)nt);
+            for_chunks(nt, nd.count, [&](int k, int64_t lo, int64_t hi) { bin_range(part[k], p0 + lo, p0 + hi); });
+            for (int k = 0; k < nt; ++k)
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < kBins; ++b) {
+                        all.bb[a][b].grow(part[k].bb[a][b]);
+                        all.bc[a][b] += part[k].bc[a][b];
                     }
+        } else {
+            bin_range(all, p0, p1);
+        }
+        const auto &bb = all.bb;
+        const auto &bc = all.bc;
+        for (int a = 0; a < 3; ++a) {
+            if (!live[a]) continue;
+            double ra[kBins];
+            int64_t rn[kBins];
+            Box acc;
+            int64_t cnt = 0;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bb[a][b]);
+                cnt += bc[a][b];
+                ra[b] = acc.area();
+                rn[b] = cnt;
+            }
+            acc = Box();
+            cnt = 0;
+            for (int b = 0; b < kBins - 1; ++b) {
+                acc.grow(bb[a][b]);
+                cnt += bc[a][b];
+                if (cnt == 0 || rn[b + 1] == 0) continue;
+                const double c = acc.area() * (double)cnt + ra[b + 1] * (double)rn[b + 1];
+                if (c < best_cost) {
+                    best_cost = c;
+                    best_axis = a;
+                    best_bin = b;
                 }
             }
-            double leaf_cost = nd.box.area() * (double)nd.count;
-            double split_cost = nd.box.area() * 1.0 + best_cost;
-            if (best_axis < 0 || (split_cost >= leaf_cost && nd.count <= kLeafMax)) make_leaf = nd.count <= kLeafMax;
         }
-        if (make_leaf) {
-            nd.leaf = true;
+        const double leaf_cost = nd.box.area() * (double)nd.count;
+        const double split_cost = nd.box.area() * 1.0 + best_cost;
+        if (best_axis < 0 || (split_cost >= leaf_cost && nd.count <= kLeafMax)) make_leaf = nd.count <= kLeafMax;
+    }
+    if (make_leaf) {
+        nd.leaf = true;
+        return false;
+    }
+    if (best_axis >= 0) {
+        const int a = best_axis;
+        const float lo = cb.lo[a];
+        const double sc = kBins / ((double)cb.hi[a] - lo);
+        Prim *it = std::partition(p0, p1, [&](const Prim &p) { return bin_of(p.c[a], lo, sc) <= best_bin; });
+        mid = nd.first + (it - p0);
+    } else {
+        mid = nd.first + nd.count / 2;  // coincident centroids: split by position in the list
+    }
+    if (mid == nd.first || mid == nd.first + nd.count) mid = nd.first + nd.count / 2;
+    return true;
+}
+
+// Builds the subtree rooted at nodes[root] (first/count set), appending its nodes.
+void build_from(Prim *pr, std::vector<BNode> &nodes, int32_t root, int leaf_target, int64_t stop_below,
+                std::vector<int32_t> *deferred, int n_threads)
+{
+    std::vector<int32_t> work{root};
+    while (!work.empty()) {
+        const int32_t ni = work.back();
+        work.pop_back();
+        if (deferred && nodes[ni].count <= stop_below) {
+            deferred->push_back(ni);
+            continue;
+        }
+        BNode nd = nodes[ni];
+        int64_t mid = 0;
+        if (!split_node(pr, nd, leaf_target, mid, n_threads)) {
             nodes[ni] = nd;
             continue;
         }
-        int64_t mid;
-        if (best_axis >= 0) {
-            float lo = cb.lo[best_axis], hi = cb.hi[best_axis];
-            const double sc = kBins / ((double)hi - lo);
-            auto it = std::partition(idx.begin() + nd.first, idx.begin() + nd.first + nd.count,
-                                     [&](int64_t t) {
-                                         int b = (int)((cen[3 * t + best_axis] - lo) * sc);
-                                         b = std::min(std::max(b, 0), kBins - 1);
-                                         return b <= best_bin;
-                                     });
-            mid = it - idx.begin();
-        } else {
-            mid = nd.first + nd.count / 2;  // coincident centroids: split by position in the list
-        }
-        if (mid == nd.first || mid == nd.first + nd.count) mid = nd.first + nd.count / 2;
         BNode l, r;
         l.first = nd.first;
         l.count = mid - nd.first;
@@ -166,6 +222,78 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
         nodes.push_back(r);
         work.push_back(nd.child[1]);
         work.push_back(nd.child[0]);
+    }
+}
+
+}  // namespace
+
+void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
+{
+    out = Bvh();
+    std::vector<Prim> pr((size_t)n);
+    Box scene;
+    double max_abs = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const float *t = tri + 9 * i;
+        Prim &p = pr[(size_t)i];
+        for (int v = 0; v < 3; ++v) {
+            p.box.grow(t + 3 * v);
+            for (int a = 0; a < 3; ++a) max_abs = std::max(max_abs, (double)std::fabs(t[3 * v + a]));
+        }
+        for (int a = 0; a < 3; ++a) p.c[a] = 0.5f * (p.box.lo[a] + p.box.hi[a]);
+        p.id = (int32_t)i;
+        scene.grow(p.box);
+    }
+    double ext = 0.0;
+    if (n > 0)
+        for (int a = 0; a < 3; ++a) ext = std::max(ext, (double)scene.hi[a] - scene.lo[a]);
+    const float margin = (float)(1e-5 * std::max(ext, max_abs) + 1e-30);
+    out.margin = margin;
+    for (int a = 0; a < 3; ++a) {
+        out.lo[a] = n ? scene.lo[a] : 0.0f;
+        out.hi[a] = n ? scene.hi[a] : 0.0f;
+    }
+
+    std::vector<BNode> nodes;
+    nodes.reserve((size_t)(2 * n / std::max(1, leaf_target) + 4));
+    nodes.push_back(BNode());
+    nodes[0].first = 0;
+    nodes[0].count = n;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int n_threads = (int)std::min(hw, 16u);
+    if (n < 32768 || n_threads == 1) {
+        build_from(pr.data(), nodes, 0, leaf_target, 0, nullptr, 1);
+    } else {
+        // split the large nodes here; defer the subtrees below the grain to the workers
+        const int64_t grain = std::max<int64_t>(4096, n / (8 * n_threads));
+        std::vector<int32_t> roots;
+        build_from(pr.data(), nodes, 0, leaf_target, grain, &roots, n_threads);
+        std::vector<std::vector<BNode>> sub(roots.size());
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t t; (t = next.fetch_add(1)) < roots.size();) {
+                std::vector<BNode> &L = sub[t];
+                L.push_back(nodes[roots[t]]);
+                build_from(pr.data(), L, 0, leaf_target, 0, nullptr, 1);
+            }
+        };
+        std::vector<std::thread> pool;
+        const int nw = (int)std::min<size_t>((size_t)n_threads, roots.size());
+        for (int k = 1; k < nw; ++k) pool.emplace_back(worker);
+        worker();
+        for (std::thread &th : pool) th.join();
+        // append each subtree; its local node 0 replaces the deferred node
+        for (size_t t = 0; t < roots.size(); ++t) {
+            const std::vector<BNode> &L = sub[t];
+            const int32_t base = (int32_t)nodes.size() - 1;
+            auto remap = [&](BNode b) {
+                for (int c = 0; c < 2; ++c)
+                    if (b.child[c] >= 0) b.child[c] += base;
+                return b;
+            };
+            nodes[roots[t]] = remap(L[0]);
+            for (size_t k = 1; k < L.size(); ++k) nodes.push_back(remap(L[k]));
+        }
     }
 
     // A root that is a leaf gets a synthetic internal parent whose two children are
@@ -226,12 +354,11 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
     out.tri_b.resize((size_t)n);
     out.tri_c.resize((size_t)n);
     for (int64_t j = 0; j < n; ++j) {
-        const int64_t o = idx[j];
-        const float *t = tri + 9 * o;
+        const int32_t oi = pr[(size_t)j].id;
+        const float *t = tri + 9 * (int64_t)oi;
         // E = K - M, F = L - M, exactly as FindTriangleInPath computes them
         float Ex = t[0] - t[6], Ey = t[1] - t[7], Ez = t[2] - t[8];
         float Fx = t[3] - t[6], Fy = t[4] - t[7], Fz = t[5] - t[8];
-        int32_t oi = (int32_t)o;
         float ob;
         std::memcpy(&ob, &oi, 4);
         out.tri_a[j] = {t[6], t[7], t[8], Ex};
