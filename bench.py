@@ -467,18 +467,21 @@ def ours_arm(args, cases):
         del flush
         torch.cuda.empty_cache()
 
-    # e2e through the public API with host buffers: every step creates a context, sets
-    # the mesh (BVH + safety grid build, upload) and the other inputs from host arrays,
-    # then for each case sets its media, runs and copies all tallies back.
+    # e2e through the public API with host buffers, on one long-lived context (as the
+    # reference's CalculatePropagation object is): every step sets the mesh (BVH build,
+    # then upload and cell-grid build at the next run) and the other inputs from host
+    # arrays, then for each case sets its media, runs and copies all tallies back.
+    # Context creation and release stay outside the timed steps: releasing a context's
+    # buffers took 0.005-2 s on this driver, varying from call to call.
     e2e_v = h2d = d2h = None
     e2e_steps = max(1, min(args.steps, 3))
     if rank == 0 or world > 1:
         e2e_t = 0.0
-        for i in range(e2e_steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            h2d = d2h = 0
-            with Simulation(local) as s2:
+        with Simulation(local) as s2:
+            for i in range(e2e_steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                h2d = d2h = 0
                 w.apply(s2, seed=0x4C50 + 1 + i)
                 for j, c in enumerate(cases):
                     if ncase > 1:
@@ -488,7 +491,7 @@ def ours_arm(args, cases):
                     h2d += s2.stats()["h2d_bytes"]
                     s2.tallies()
                     d2h += s2.stats()["d2h_bytes"]
-            e2e_t += time.perf_counter() - t0
+                e2e_t += time.perf_counter() - t0
         e2e_v = n * ncase * world * e2e_steps / e2e_t
 
     if dist is not None:

@@ -34,8 +34,8 @@ cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *ori
                          cudaStream_t s);
 cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out,
                           cudaStream_t s);
-cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, uint16_t *out,
-                               cudaStream_t s);
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *coarse,
+                               uint16_t *out, cudaStream_t s);
 cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, uint32_t *count, const uint32_t *start,
                               int32_t *refs, cudaStream_t s);
 cudaError_t launch_cell_words(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start, bool lists,
@@ -77,6 +77,40 @@ struct DevBuf {
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
+};
+
+// Page-locked host memory, so that the tally copies run at the link's speed rather than
+// through the driver's staging buffer.  size() is the last resize; the allocation grows.
+template <class T>
+struct HostBuf {
+    T *p = nullptr;
+    size_t n = 0, cap = 0;
+    cudaError_t resize(size_t count)
+    {
+        if (count > cap) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            cap = n = 0;
+            cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&p), count * sizeof(T), cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                return e;
+            }
+            cap = count;
+        }
+        n = count;
+        return cudaSuccess;
+    }
+    T *data() { return p; }
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    HostBuf() = default;
+    HostBuf(const HostBuf &) = delete;
+    HostBuf &operator=(const HostBuf &) = delete;
+    ~HostBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
 };
 
 // Ring signals and their derivatives formed from the device sums (see KParams::grad).
@@ -190,7 +224,7 @@ struct lp_ctx {
     std::vector<double> h_grad;
     GradOut gout;
     // host copies of tallies
-    std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
+    HostBuf<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det;
     float last_ms = 0.0f;
     bool launched = false;
     // statistics
@@ -484,7 +518,8 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
 
 // Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
 // the grid has at most grid_max_cells cells; safety bounds in units of h / 256.
-//   1. safety_grid_kernel: per cell, a lower bound of the distance to the nearest triangle;
+//   1. safety_coarse_kernel, safety_grid_kernel: per cell, a lower bound of the distance
+//      to the nearest triangle (blocks of 2 x 2 x 2 cells first, to bound each cell's search);
 //   2. cell_lists_kernel (count pass): per cell, the triangles touching it;
 //   3. exclusive scan of the counts: each cell's first slot in cell_refs;
 //   4. cell_lists_kernel (fill pass): the triangle indices;
@@ -525,6 +560,7 @@ int build_safety_grid(lp_ctx *c)
     c->g_eps = (float)(2e-5 * scale);
     for (int a = 0; a < 3; ++a) c->g_origin[a] = (float)(b.lo[a] - h);
     DevBuf<uint16_t> safe;
+    DevBuf<float> coarse;
     DevBuf<uint32_t> count, start;
     DevBuf<unsigned char> scan_tmp;
     LP_CUDA(c, safe.ensure((size_t)cells));
@@ -544,8 +580,10 @@ int build_safety_grid(lp_ctx *c)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    cudaError_t e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h),
-                                           safe.p, s);
+    cudaError_t e = coarse.ensure((size_t)((c->g_n[0] + 1) / 2) * ((c->g_n[1] + 1) / 2) * ((c->g_n[2] + 1) / 2));
+    if (e == cudaSuccess)
+        e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h), coarse.p,
+                                   safe.p, s);
     bool lists = false;
     if (e == cudaSuccess && c->cell_lists) {
         const int nt = (int)c->bvh.tri_a.size();
@@ -974,13 +1012,13 @@ int lp_get_tallies(lp_ctx *c, lp_tallies *out)
     if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_tallies: NULL argument");
     if (c->tally_dirty || !c->sft.p) return fail(c, LP_ERR_STATE, "lp_get_tallies: nothing has run");
     const lp_geometry &g = c->geo;
-    c->h_sft.resize((size_t)g.sft_nx * g.sft_ny * 3);
-    c->h_rtd.resize((size_t)g.dimR * g.dimAlpha * 3);
-    c->h_rz.resize((size_t)g.rz_nr * g.rz_nz * 2);
-    c->h_vox.resize((size_t)n_vox(c));
-    c->h_rbins.resize((size_t)c->n_rbins * 2);
-    c->h_region.resize((size_t)c->n_media);
-    c->h_det.resize(c->det_r.size());
+    LP_CUDA(c, c->h_sft.resize((size_t)g.sft_nx * g.sft_ny * 3));
+    LP_CUDA(c, c->h_rtd.resize((size_t)g.dimR * g.dimAlpha * 3));
+    LP_CUDA(c, c->h_rz.resize((size_t)g.rz_nr * g.rz_nz * 2));
+    LP_CUDA(c, c->h_vox.resize((size_t)n_vox(c)));
+    LP_CUDA(c, c->h_rbins.resize((size_t)c->n_rbins * 2));
+    LP_CUDA(c, c->h_region.resize((size_t)c->n_media));
+    LP_CUDA(c, c->h_det.resize(c->det_r.size()));
     cudaStream_t s = c->stream;
     LP_CUDA(c, cudaMemcpyAsync(c->h_sft.data(), c->sft.p, c->h_sft.size() * 8, cudaMemcpyDeviceToHost, s));
     LP_CUDA(c, cudaMemcpyAsync(c->h_rtd.data(), c->rtd.p, c->h_rtd.size() * 8, cudaMemcpyDeviceToHost, s));

@@ -105,30 +105,80 @@ __device__ float nearest_dist2(const KParams &P, V3 p, float cap2)
     return best;
 }
 
+// First pass: distance from the centre of each block of 2 x 2 x 2 cells to the nearest
+// triangle, capped at cap_c.
+__global__ void __launch_bounds__(256) safety_coarse_kernel(const __grid_constant__ KParams P, float h, float cap_c,
+                                                            float *dist)
+{
+    const int cx = (P.g_nx + 1) / 2, cy = (P.g_ny + 1) / 2, cz = (P.g_nz + 1) / 2;
+    const int64_t n = (int64_t)cx * cy * cz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int jx = (int)(i % cx);
+        const int jy = (int)((i / cx) % cy);
+        const int jz = (int)(i / ((int64_t)cx * cy));
+        const V3 c = v3(P.g_ox + (float)(2 * jx + 1) * h, P.g_oy + (float)(2 * jy + 1) * h,
+                        P.g_oz + (float)(2 * jz + 1) * h);
+        dist[i] = sqrtf(nearest_dist2(P, c, cap_c * cap_c));
+    }
+}
+
+// Second pass, per cell.  A cell centre lies off = sqrt(3)/2 h from its block's centre,
+// so its distance d is within dc +- off of the block's distance dc.  The cell's nearest-
+// triangle search therefore starts from the bound dc + off (plus rounding margins)
+// instead of cap, which prunes most of the tree at once, and is skipped when
+// dc - off exceeds cap.  Both give the value the search with cap returns, bit for bit:
+// min(cap^2, nearest squared distance).  coarse == nullptr: one pass, every search from cap.
 __global__ void __launch_bounds__(256) safety_grid_kernel(const __grid_constant__ KParams P, float h,
                                                           float half_diag, float eps, float cap,
-                                                          uint16_t *out)
+                                                          const float *coarse, uint16_t *out)
 {
     const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
+    const int cx = (P.g_nx + 1) / 2, cy = (P.g_ny + 1) / 2;
     const float inv_unit = 1.0f / P.g_unit;
+    const float cap2 = cap * cap;
+    const float off = 0.8660254f * h, tol = 1e-3f * h;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int ix = (int)(i % P.g_nx);
         const int iy = (int)((i / P.g_nx) % P.g_ny);
         const int iz = (int)(i / ((int64_t)P.g_nx * P.g_ny));
         const V3 c = v3(P.g_ox + (ix + 0.5f) * h, P.g_oy + (iy + 0.5f) * h, P.g_oz + (iz + 0.5f) * h);
-        const float d = sqrtf(nearest_dist2(P, c, cap * cap));
+        float best2;
+        if (coarse) {
+            const float dc = coarse[((int64_t)(iz >> 1) * cy + (iy >> 1)) * cx + (ix >> 1)];
+            const float lb = (dc - off) * (1.0f - 1e-5f) - tol;
+            const float ub = (dc + off) * (1.0f + 1e-5f) + tol;
+            if (lb > cap) {
+                best2 = cap2;
+            } else if (ub < cap) {
+                const float ub2 = ub * ub;
+                best2 = nearest_dist2(P, c, ub2);
+                if (!(best2 < ub2)) best2 = nearest_dist2(P, c, cap2);   // not reached: dc + off bounds d
+            } else {
+                best2 = nearest_dist2(P, c, cap2);
+            }
+        } else {
+            best2 = nearest_dist2(P, c, cap2);
+        }
+        const float d = sqrtf(best2);
         const float safe = (d - half_diag - eps) * 0.9999f;
         float q = safe > 0.0f ? floorf(safe * inv_unit) : 0.0f;
         out[i] = (uint16_t)fminf(q, 65535.0f);
     }
 }
 
-cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, uint16_t *out,
-                               cudaStream_t s)
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *coarse,
+                               uint16_t *out, cudaStream_t s)
 {
+    if (coarse) {
+        const int64_t nc = (int64_t)((P.g_nx + 1) / 2) * ((P.g_ny + 1) / 2) * ((P.g_nz + 1) / 2);
+        const int gc = (int)std::min<int64_t>((nc + 255) / 256, 148 * 16);
+        // the block distance is exact up to cap + off and beyond it only needs to exceed that
+        safety_coarse_kernel<<<std::max(gc, 1), 256, 0, s>>>(P, h, (cap + 0.8660254f * h) * 1.001f + 0.01f * h,
+                                                             coarse);
+    }
     const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
     const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
-    safety_grid_kernel<<<std::max(grid, 1), 256, 0, s>>>(P, h, half_diag, eps, cap, out);
+    safety_grid_kernel<<<std::max(grid, 1), 256, 0, s>>>(P, h, half_diag, eps, cap, coarse, out);
     return cudaGetLastError();
 }
 
