@@ -34,8 +34,8 @@ cudaError_t launch_query(const KParams &P, int smem, int64_t n, const float *ori
                          cudaStream_t s);
 cudaError_t launch_philox(const uint32_t *ctr, const uint32_t *key, int64_t n, uint32_t *out,
                           cudaStream_t s);
-cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *coarse,
-                               uint16_t *out, cudaStream_t s);
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *const *levels,
+                               int n_levels, uint16_t *out, cudaStream_t s);
 cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, uint32_t *count, const uint32_t *start,
                               int32_t *refs, cudaStream_t s);
 cudaError_t launch_cell_words(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start, bool lists,
@@ -518,8 +518,8 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
 
 // Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
 // the grid has at most grid_max_cells cells; safety bounds in units of h / 256.
-//   1. safety_coarse_kernel, safety_grid_kernel: per cell, a lower bound of the distance
-//      to the nearest triangle (blocks of 2 x 2 x 2 cells first, to bound each cell's search);
+//   1. safety_level_kernel: per cell, a lower bound of the distance to the nearest
+//      triangle, from blocks of 8, 4 and 2 cells per edge down to cells;
 //   2. cell_lists_kernel (count pass): per cell, the triangles touching it;
 //   3. exclusive scan of the counts: each cell's first slot in cell_refs;
 //   4. cell_lists_kernel (fill pass): the triangle indices;
@@ -560,7 +560,7 @@ int build_safety_grid(lp_ctx *c)
     c->g_eps = (float)(2e-5 * scale);
     for (int a = 0; a < 3; ++a) c->g_origin[a] = (float)(b.lo[a] - h);
     DevBuf<uint16_t> safe;
-    DevBuf<float> coarse;
+    DevBuf<float> level[4];   // block distances of the safety grid's levels 1..3
     DevBuf<uint32_t> count, start;
     DevBuf<unsigned char> scan_tmp;
     LP_CUDA(c, safe.ensure((size_t)cells));
@@ -580,9 +580,21 @@ int build_safety_grid(lp_ctx *c)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    cudaError_t e = coarse.ensure((size_t)((c->g_n[0] + 1) / 2) * ((c->g_n[1] + 1) / 2) * ((c->g_n[2] + 1) / 2));
+    // levels of blocks of 2, 4 and 8 cells per edge above the cells (fewer on small grids)
+    int n_levels = 0;
+    cudaError_t e = cudaSuccess;
+    float *lv[4] = {nullptr, nullptr, nullptr, nullptr};
+    while (n_levels < 3 && e == cudaSuccess) {
+        const int L = n_levels + 1;
+        const int64_t nb = (int64_t)((c->g_n[0] + (1 << L) - 1) >> L) * ((c->g_n[1] + (1 << L) - 1) >> L) *
+                           ((c->g_n[2] + (1 << L) - 1) >> L);
+        if (nb < 512) break;
+        e = level[L].ensure((size_t)nb);
+        lv[L] = level[L].p;
+        ++n_levels;
+    }
     if (e == cudaSuccess)
-        e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h), coarse.p,
+        e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h), lv, n_levels,
                                    safe.p, s);
     bool lists = false;
     if (e == cudaSuccess && c->cell_lists) {

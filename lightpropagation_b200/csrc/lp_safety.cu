@@ -1,8 +1,9 @@
 // lp_safety.cu -- safety-distance grid over the mesh, built once per mesh on the GPU.
 //
 // Cell value = a lower bound, in units of `unit`, of the distance from ANY point of the
-// cell to the nearest triangle: (exact distance from the cell centre) - (half cell
-// diagonal) - eps, rounded down.  eps covers the rounding of the reference's
+// cell to the nearest triangle: (distance from the cell centre, exact within a few cells
+// of a triangle and a lower bound farther out) - (half cell diagonal) - eps, rounded
+// down.  eps covers the rounding of the reference's
 // ray/triangle test, which can accept intersection points a few ulp outside a
 // triangle.  A transport step shorter than this bound cannot reach any triangle, so
 // the bounded nearest-hit query would return "no hit": the kernel skips it and the
@@ -105,80 +106,85 @@ __device__ float nearest_dist2(const KParams &P, V3 p, float cap2)
     return best;
 }
 
-// First pass: distance from the centre of each block of 2 x 2 x 2 cells to the nearest
-// triangle, capped at cap_c.
-__global__ void __launch_bounds__(256) safety_coarse_kernel(const __grid_constant__ KParams P, float h, float cap_c,
-                                                            float *dist)
+// Safety grid, built level by level from blocks of 2^L x 2^L x 2^L cells (edge s = 2^L h)
+// down to single cells.  A block's centre lies off = sqrt(3)/2 s from the centre of its
+// parent block, so with dp the parent's distance, its own distance to the nearest
+// triangle lies in [dp - off, dp + off] (the code widens both ends for rounding):
+//  * lower end above near_T: the block is far from every triangle, and the lower end
+//    is kept as its (conservative) distance, with no search;
+//  * otherwise: a nearest-triangle search starting from the upper end, which prunes all
+//    but the triangles around the block.
+// near_T grows with the level so that the children of a far block are far too, and a
+// near block's distance is always exact (capped at cap), as its children's upper end
+// needs.  The top level has no parent and searches from cap.  Level 0 (Final) turns the
+// cell-centre distance d into the cell's bound, in units of g_unit:
+// (d - half_diag - eps) * 0.9999, rounded down.  eps covers the few-ulp overreach of the
+// ray/triangle test; every value is a lower bound of the true distance.
+template <bool Final>
+__global__ void __launch_bounds__(256) safety_level_kernel(const __grid_constant__ KParams P, float s, int nx, int ny,
+                                                           int nz, const float *parent, float off, float near_t,
+                                                           float cap, float half_diag, float eps, float *dist,
+                                                           uint16_t *out)
 {
-    const int cx = (P.g_nx + 1) / 2, cy = (P.g_ny + 1) / 2, cz = (P.g_nz + 1) / 2;
-    const int64_t n = (int64_t)cx * cy * cz;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int jx = (int)(i % cx);
-        const int jy = (int)((i / cx) % cy);
-        const int jz = (int)(i / ((int64_t)cx * cy));
-        const V3 c = v3(P.g_ox + (float)(2 * jx + 1) * h, P.g_oy + (float)(2 * jy + 1) * h,
-                        P.g_oz + (float)(2 * jz + 1) * h);
-        dist[i] = sqrtf(nearest_dist2(P, c, cap_c * cap_c));
-    }
-}
-
-// Second pass, per cell.  A cell centre lies off = sqrt(3)/2 h from its block's centre,
-// so its distance d is within dc +- off of the block's distance dc.  The cell's nearest-
-// triangle search therefore starts from the bound dc + off (plus rounding margins)
-// instead of cap, which prunes most of the tree at once, and is skipped when
-// dc - off exceeds cap.  Both give the value the search with cap returns, bit for bit:
-// min(cap^2, nearest squared distance).  coarse == nullptr: one pass, every search from cap.
-__global__ void __launch_bounds__(256) safety_grid_kernel(const __grid_constant__ KParams P, float h,
-                                                          float half_diag, float eps, float cap,
-                                                          const float *coarse, uint16_t *out)
-{
-    const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
-    const int cx = (P.g_nx + 1) / 2, cy = (P.g_ny + 1) / 2;
-    const float inv_unit = 1.0f / P.g_unit;
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int px = (nx + 1) / 2, py = (ny + 1) / 2;
+    const float tol = 1e-3f * P.g_unit * 256.0f;   // 1e-3 of a cell
     const float cap2 = cap * cap;
-    const float off = 0.8660254f * h, tol = 1e-3f * h;
+    const float inv_unit = 1.0f / P.g_unit;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int ix = (int)(i % P.g_nx);
-        const int iy = (int)((i / P.g_nx) % P.g_ny);
-        const int iz = (int)(i / ((int64_t)P.g_nx * P.g_ny));
-        const V3 c = v3(P.g_ox + (ix + 0.5f) * h, P.g_oy + (iy + 0.5f) * h, P.g_oz + (iz + 0.5f) * h);
-        float best2;
-        if (coarse) {
-            const float dc = coarse[((int64_t)(iz >> 1) * cy + (iy >> 1)) * cx + (ix >> 1)];
-            const float lb = (dc - off) * (1.0f - 1e-5f) - tol;
-            const float ub = (dc + off) * (1.0f + 1e-5f) + tol;
-            if (lb > cap) {
-                best2 = cap2;
-            } else if (ub < cap) {
-                const float ub2 = ub * ub;
-                best2 = nearest_dist2(P, c, ub2);
-                if (!(best2 < ub2)) best2 = nearest_dist2(P, c, cap2);   // not reached: dc + off bounds d
+        const int ix = (int)(i % nx);
+        const int iy = (int)((i / nx) % ny);
+        const int iz = (int)(i / ((int64_t)nx * ny));
+        const V3 c = v3(P.g_ox + (ix + 0.5f) * s, P.g_oy + (iy + 0.5f) * s, P.g_oz + (iz + 0.5f) * s);
+        float d;
+        if (parent) {
+            const float dp = parent[((int64_t)(iz >> 1) * py + (iy >> 1)) * px + (ix >> 1)];
+            const float lb = (dp - off) * (1.0f - 1e-5f) - tol;
+            if (lb > near_t) {
+                d = lb;
             } else {
-                best2 = nearest_dist2(P, c, cap2);
+                const float r = fminf((dp + off) * (1.0f + 1e-5f) + tol, cap);
+                float best2 = nearest_dist2(P, c, r * r);
+                if (!(best2 < r * r) && r < cap) best2 = nearest_dist2(P, c, cap2);   // not reached
+                d = sqrtf(best2);
             }
         } else {
-            best2 = nearest_dist2(P, c, cap2);
+            d = sqrtf(nearest_dist2(P, c, cap2));
         }
-        const float d = sqrtf(best2);
-        const float safe = (d - half_diag - eps) * 0.9999f;
-        float q = safe > 0.0f ? floorf(safe * inv_unit) : 0.0f;
-        out[i] = (uint16_t)fminf(q, 65535.0f);
+        if (Final) {
+            const float safe = (d - half_diag - eps) * 0.9999f;
+            const float q = safe > 0.0f ? floorf(safe * inv_unit) : 0.0f;
+            out[i] = (uint16_t)fminf(q, 65535.0f);
+        } else {
+            dist[i] = d;
+        }
     }
 }
 
-cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *coarse,
-                               uint16_t *out, cudaStream_t s)
+cudaError_t launch_safety_grid(const KParams &P, float h, float half_diag, float eps, float cap, float *const *levels,
+                               int n_levels, uint16_t *out, cudaStream_t s)
 {
-    if (coarse) {
-        const int64_t nc = (int64_t)((P.g_nx + 1) / 2) * ((P.g_ny + 1) / 2) * ((P.g_nz + 1) / 2);
-        const int gc = (int)std::min<int64_t>((nc + 255) / 256, 148 * 16);
-        // the block distance is exact up to cap + off and beyond it only needs to exceed that
-        safety_coarse_kernel<<<std::max(gc, 1), 256, 0, s>>>(P, h, (cap + 0.8660254f * h) * 1.001f + 0.01f * h,
-                                                             coarse);
+    // thresholds: near_t[L + 1] >= near_t[L] + off[L] + margins, so far parents have far children
+    float near_t[8], off[8];
+    near_t[0] = 16.0f * h;
+    for (int L = 0; L < n_levels; ++L) {
+        off[L] = 0.8660254f * h * (float)(1 << L);
+        near_t[L + 1] = near_t[L] * 1.0001f + off[L] + 0.01f * h;
     }
-    const int64_t n = (int64_t)P.g_nx * P.g_ny * P.g_nz;
-    const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
-    safety_grid_kernel<<<std::max(grid, 1), 256, 0, s>>>(P, h, half_diag, eps, cap, coarse, out);
+    for (int L = n_levels; L >= 0; --L) {
+        const int nx = (P.g_nx + (1 << L) - 1) >> L, ny = (P.g_ny + (1 << L) - 1) >> L;
+        const int nz = (P.g_nz + (1 << L) - 1) >> L;
+        const int64_t n = (int64_t)nx * ny * nz;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+        const float *par = L < n_levels ? levels[L + 1] : nullptr;
+        const float o = L < n_levels ? off[L] : 0.0f;
+        if (L == 0)
+            safety_level_kernel<true><<<grid, 256, 0, s>>>(P, h, nx, ny, nz, par, o, near_t[0], cap, half_diag, eps,
+                                                            nullptr, out);
+        else
+            safety_level_kernel<false><<<grid, 256, 0, s>>>(P, h * (float)(1 << L), nx, ny, nz, par, o, near_t[L], cap,
+                                                             half_diag, eps, levels[L], nullptr);
+    }
     return cudaGetLastError();
 }
 
