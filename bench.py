@@ -459,40 +459,41 @@ def ours_arm(args, cases):
                     "derivatives": int(sim._rings.shape[0] * (cases[0].nmuasg.shape[0] - 1) * 2 * ncase),
                     "what": "one launch per case giving d(ring signal)/d(mua, mus) of every region and ring"}
 
+    # e2e through the public API with host buffers, on the long-lived context of the
+    # timed steps (as the reference's CalculatePropagation object is long-lived): every
+    # step sets the mesh (BVH build, then upload and cell-grid build at the next run) and
+    # the other inputs from host arrays, then for each case sets its media, runs and
+    # copies all tallies back.  Creating and releasing a context stays outside: the
+    # release of a context's buffers took 0.005-2 s on this driver, and the same launch
+    # ran up to 30 % slower in a context whose buffers the driver placed after other
+    # large allocations.  transport_ms_per_step is the device time of the step's launches.
+    e2e_v = h2d = d2h = e2e_dev_ms = None
+    e2e_steps = max(1, min(args.steps, 3))
+    if rank == 0 or world > 1:
+        e2e_t, e2e_dev_ms = 0.0, 0.0
+        for i in range(e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h2d = d2h = 0
+            w.apply(sim, seed=0x4C50 + 1 + i)
+            for j, c in enumerate(cases):
+                if ncase > 1:
+                    sim.set_media(c.nmuasg)
+                sim.zero()
+                sim.run(n, (rank * ncase + j) * n)
+                h2d += sim.stats()["h2d_bytes"]
+                sim.tallies()
+                d2h += sim.stats()["d2h_bytes"]
+                e2e_dev_ms += sim.kernel_ms()
+            e2e_t += time.perf_counter() - t0
+        e2e_v = n * ncase * world * e2e_steps / e2e_t
+        e2e_dev_ms /= e2e_steps
     if dist is None:
-        # release the timed context and the flush buffer, so that each e2e context is
-        # allocated like the first context of a process (see the flush buffer above)
+        # the batched section's contexts are allocated after this one is released
         sim.close()
         sim = None
         del flush
         torch.cuda.empty_cache()
-
-    # e2e through the public API with host buffers, on one long-lived context (as the
-    # reference's CalculatePropagation object is): every step sets the mesh (BVH build,
-    # then upload and cell-grid build at the next run) and the other inputs from host
-    # arrays, then for each case sets its media, runs and copies all tallies back.
-    # Context creation and release stay outside the timed steps: releasing a context's
-    # buffers took 0.005-2 s on this driver, varying from call to call.
-    e2e_v = h2d = d2h = None
-    e2e_steps = max(1, min(args.steps, 3))
-    if rank == 0 or world > 1:
-        e2e_t = 0.0
-        with Simulation(local) as s2:
-            for i in range(e2e_steps):
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                h2d = d2h = 0
-                w.apply(s2, seed=0x4C50 + 1 + i)
-                for j, c in enumerate(cases):
-                    if ncase > 1:
-                        s2.set_media(c.nmuasg)
-                    s2.zero()
-                    s2.run(n, (rank * ncase + j) * n)
-                    h2d += s2.stats()["h2d_bytes"]
-                    s2.tallies()
-                    d2h += s2.stats()["d2h_bytes"]
-                e2e_t += time.perf_counter() - t0
-        e2e_v = n * ncase * world * e2e_steps / e2e_t
 
     if dist is not None:
         red.clear()
@@ -560,7 +561,8 @@ def ours_arm(args, cases):
                        "grid": st["grid"], "block": st["block"], "bvh_nodes": st["n_nodes"],
                        "bvh_nodes_in_smem": st["nodes_smem"], "tris_in_smem": st["tris_smem"]},
             "wall_s": wall, "clocks": clk, "gpu_launches": args.steps * ncase,
-            "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "transport_ms_per_step": e2e_dev_ms},
             "detector_error": rse, "gradient": gradient, "batched": batched,
             "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line))

@@ -212,7 +212,7 @@ int lp_batch_get_gradient(lp_batch *b, int32_t inst, lp_gradient *out);
 
 /* Shared memory per block (bytes) for BVH nodes and triangles staged by the transport
  * kernel; what a block does not take stays L1 cache for the cell grid, tallies and the
- * rest of the mesh.  No reference counterpart; results do not depend on it. */
+ * rest of the mesh.  Default 8192.  No reference counterpart; results do not depend on it. */
 int lp_set_smem_budget(lp_ctx *ctx, int32_t bytes);
 /* Whether cells touched by triangles list them (1, default) or hold no information
  * (0: every query that the safety bound does not skip descends the BVH).  Results are

@@ -208,7 +208,10 @@ struct lp_ctx {
     DevBuf<unsigned long long> sft, rtd, rz, vox, rbins, region, det, counters, work;
     DevBuf<float> exit_rec;
     // safety grid (lp_set_safety_grid)
-    int smem_budget = 64 * 1024;   // shared memory per block for staged BVH nodes and triangles
+    // shared memory per block for staged BVH nodes and triangles: 8 KB stages a small mesh whole,
+    // and on a large one the L1 left over (the cell grid, lists, triangles) is worth more than
+    // the staged top of the tree (64 KB measured 1.2 % slower on the 202,500-triangle abdomen)
+    int smem_budget = 8 * 1024;
     int64_t grid_max_cells = int64_t(1) << 24;
     bool grid_dirty = true;
     bool cell_lists = true;
