@@ -223,12 +223,17 @@ __device__ bool tri_cube_overlap(V3 c, float r, V3 a, V3 b, V3 d)
 
 // One pass over the triangles (BVH order): every cell that a triangle touches (cells
 // widened by eps) gets a count (refs == nullptr) or, in the second pass, the triangle's
-// index at start[cell] + the next free slot (count re-zeroed before that pass).
+// index at start[cell] + the next free slot (count re-zeroed before that pass).  One warp
+// per triangle, its lanes striding over the cells of the triangle's box: a large
+// triangle (a slab face covers 10^5 cells) is not left to a single thread.  The order of
+// the entries within a cell is not defined, and no query depends on it.
 __global__ void __launch_bounds__(256) cell_lists_kernel(const __grid_constant__ KParams P, int n_tri, float h,
                                                          float eps, uint32_t *count, const uint32_t *start,
                                                          int32_t *refs)
 {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_tri; j += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int n_warps = (gridDim.x * blockDim.x) >> 5;
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n_tri; j += n_warps) {
         const float4 ta = __ldg(P.tri_a + j), tb = __ldg(P.tri_b + j), tc = __ldg(P.tri_c + j);
         const V3 a = v3(ta.x, ta.y, ta.z);
         const V3 b = add3(a, v3(ta.w, tb.x, tb.y)), d = add3(a, v3(tb.z, tb.w, tc.x));
@@ -241,16 +246,18 @@ __global__ void __launch_bounds__(256) cell_lists_kernel(const __grid_constant__
             c0[k] = min(max((int)floorf((lo[k] - eps - o[k]) * P.g_inv_h), 0), n[k] - 1);
             c1[k] = min(max((int)floorf((hi[k] + eps - o[k]) * P.g_inv_h), 0), n[k] - 1);
         }
-        for (int z = c0[2]; z <= c1[2]; ++z)
-            for (int y = c0[1]; y <= c1[1]; ++y)
-                for (int x = c0[0]; x <= c1[0]; ++x) {
-                    const V3 c = v3(o[0] + ((float)x + 0.5f) * h, o[1] + ((float)y + 0.5f) * h,
-                                    o[2] + ((float)z + 0.5f) * h);
-                    if (!tri_cube_overlap(c, 0.5f * h + eps, a, b, d)) continue;
-                    const int64_t cell = ((int64_t)z * n[1] + y) * n[0] + x;
-                    const uint32_t k = atomicAdd(count + cell, 1u);
-                    if (refs) refs[start[cell] + k] = j;
-                }
+        const int ex = c1[0] - c0[0] + 1, ey = c1[1] - c0[1] + 1;
+        const int64_t n_cells = (int64_t)ex * ey * (c1[2] - c0[2] + 1);
+        for (int64_t q = lane; q < n_cells; q += 32) {
+            const int x = c0[0] + (int)(q % ex);
+            const int y = c0[1] + (int)((q / ex) % ey);
+            const int z = c0[2] + (int)(q / ((int64_t)ex * ey));
+            const V3 c = v3(o[0] + ((float)x + 0.5f) * h, o[1] + ((float)y + 0.5f) * h, o[2] + ((float)z + 0.5f) * h);
+            if (!tri_cube_overlap(c, 0.5f * h + eps, a, b, d)) continue;
+            const int64_t cell = ((int64_t)z * n[1] + y) * n[0] + x;
+            const uint32_t k = atomicAdd(count + cell, 1u);
+            if (refs) refs[start[cell] + k] = j;
+        }
     }
 }
 
@@ -272,7 +279,7 @@ __global__ void cell_word_kernel(int64_t n, const uint16_t *safe, const uint32_t
 cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, uint32_t *count, const uint32_t *start,
                               int32_t *refs, cudaStream_t s)
 {
-    const int grid = std::max(1, std::min((n_tri + 255) / 256, 148 * 16));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n_tri * 32 + 255) / 256, 148 * 16));
     cell_lists_kernel<<<grid, 256, 0, s>>>(P, n_tri, h, eps, count, start, refs);
     return cudaGetLastError();
 }
