@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <thread>
 
 namespace lp {
@@ -65,11 +66,19 @@ inline int bin_of(float x, float lo, double sc)
 }
 
 // Runs fn(k, lo, hi) over nt contiguous chunks of [0, n), chunk 0 on the calling thread.
+// A chunk whose thread cannot be started runs on the calling thread instead (the build is
+// called through the C ABI, where no exception may escape).
 template <class Fn>
 void for_chunks(int nt, int64_t n, Fn fn)
 {
     std::vector<std::thread> pool;
-    for (int k = 1; k < nt; ++k) pool.emplace_back([&, k]() { fn(k, n * k / nt, n * (k + 1) / nt); });
+    for (int k = 1; k < nt; ++k) {
+        try {
+            pool.emplace_back([&, k]() { fn(k, n * k / nt, n * (k + 1) / nt); });
+        } catch (const std::exception &) {
+            fn(k, n * k / nt, n * (k + 1) / nt);
+        }
+    }
     fn(0, 0, n / nt);
     for (std::thread &th : pool) th.join();
 }
@@ -279,7 +288,13 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
         };
         std::vector<std::thread> pool;
         const int nw = (int)std::min<size_t>((size_t)n_threads, roots.size());
-        for (int k = 1; k < nw; ++k) pool.emplace_back(worker);
+        for (int k = 1; k < nw; ++k) {
+            try {
+                pool.emplace_back(worker);
+            } catch (const std::exception &) {
+                break;   // the threads started so far and this one share the subtrees
+            }
+        }
         worker();
         for (std::thread &th : pool) th.join();
         // append each subtree; its local node 0 replaces the deferred node

@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -719,9 +720,19 @@ int lp_set_mesh(lp_ctx *c, int64_t n_tri, const float *tri, const float *nrm, co
         if (med[i] < 0 || med[i] >= lp::kMaxMedia)
             return fail(c, LP_ERR_INVALID, "lp_set_mesh: region id %d of triangle %lld out of range", med[i],
                         (long long)(i / 2));
-    lp::build_bvh(tri, n_tri, c->bvh);
-    if (c->bvh.depth >= lp::kStackDepth)
+    try {
+        lp::build_bvh(tri, n_tri, c->bvh);
+    } catch (const std::bad_alloc &) {
+        // the context holds no usable mesh until the next successful lp_set_mesh
+        c->bvh = lp::Bvh();
+        c->have_mesh = false;
+        return fail(c, LP_ERR_NOMEM, "lp_set_mesh: out of host memory building the BVH of %lld triangles",
+                    (long long)n_tri);
+    }
+    if (c->bvh.depth >= lp::kStackDepth) {
+        c->have_mesh = false;
         return fail(c, LP_ERR_RANGE, "lp_set_mesh: BVH depth %d exceeds the traversal stack", c->bvh.depth);
+    }
     c->tri_attr.resize((size_t)n_tri);
     for (int64_t i = 0; i < n_tri; ++i) {
         // nv = normalize(vload3(triID, normals)) (.cl:1489), done once here
