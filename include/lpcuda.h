@@ -272,9 +272,9 @@ int lp_fp32_peak(int device, double *tflops);
 
 /* --- transport without device allocation ------------------------------------- */
 /* No counterpart in the reference.  For callers that must not allocate device memory
- * through this library: code running while a stream is being captured into a CUDA
- * graph, or a host application whose device memory comes from its own pool or arena
- * with a fixed budget.  lp_run_noalloc traces photons [first, first + n_photons) with
+ * through this library: a host application whose device memory comes from its own
+ * pool or arena with a fixed budget, or code that cannot afford the device-wide
+ * synchronisation that cudaFree implies.  lp_run_noalloc traces photons [first, first + n_photons) with
  * the reference-arithmetic transport kernel and never calls cudaMalloc or cudaFree.
  * Its scratch (photon counter, event counters, media table and a small BVH built on
  * the device from the mesh arrays) lives in one static device array of

@@ -1,8 +1,8 @@
 // lp_noalloc.cu -- lp_run_noalloc: photon transport without any device allocation.
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a stream is
-// captured into a CUDA graph, or an application whose device memory comes from its
-// own arena with a fixed budget.  This entry point gives them the transport with all
+// Some callers cannot let a library call cudaMalloc: an application whose device memory
+// comes from its own arena with a fixed budget, or code that cannot afford the
+// device-wide synchronisation that cudaFree implies.  This entry point gives them the transport with all
 // scratch in the file-scope array below, so it allocates nothing; the caller passes
 // the mesh and the output tallies in its own device memory.
 //

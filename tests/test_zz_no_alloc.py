@@ -1,8 +1,8 @@
 """lp_run_noalloc: transport that allocates no device memory, against lp_run.
 
-Some callers cannot let a library call cudaMalloc: code that runs while its stream is
-being captured into a CUDA graph, or an application that hands out device memory from
-its own fixed arena.  lp_run_noalloc serves them: the caller owns every input and
+Some callers cannot let a library call cudaMalloc: an application that hands out device
+memory from its own fixed arena, or code that cannot afford the device-wide
+synchronisation that cudaFree implies.  lp_run_noalloc serves them: the caller owns every input and
 output buffer, and the entry point keeps its scratch in a static device array.
 
 Here the test plays that caller: it allocates the mesh and the output tallies itself
