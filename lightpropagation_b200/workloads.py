@@ -232,6 +232,10 @@ def batched_abdomen(n_instances: int = 512, budget=(1e6, 1e8), n_variants: int =
         depth = float(np.round(rng.uniform(30.0, 70.0), 1))
         lo = float(np.round(rng.uniform(5.0, 15.0), 1))
         hi = float(np.round(min(25.0, lo + rng.uniform(5.0, 10.0)), 1))
+        # the head must clear the uterine wall (skin 2 + fat up to hi + uterus 10 mm) by 2 mm;
+        # a shallower draw is redrawn (none is for the default seed)
+        while depth < 2.0 + hi + 10.0 + 2.0:
+            depth = float(np.round(rng.uniform(30.0, 70.0), 1))
         meshes_.append(curved_abdomen(wavelength=660, freq=variant_freq, head_depth=depth, fat=(lo, hi)))
     out, first = [], 0
     for i in range(n_instances):

@@ -84,3 +84,25 @@ def test_workload_triangle_counts():
     assert 6 * 20 * 129 ** 2 == 1_996_920
     tri, _, med = meshes.curved_abdomen(freq=45)
     assert tri.shape == (202_500, 9) and med.shape == (202_500, 2)
+
+
+def test_batched_workload_spec():
+    """The batched workload's draws follow its specification, its photon ranges tile one
+    id range, and every head variant clears the uterine wall."""
+    from lightpropagation_b200 import workloads
+    spec = workloads.batched_abdomen(n_instances=64, freq=8, variant_freq=12)
+    assert len(spec.meshes) == 9
+    inst = spec.instances
+    first = 0
+    for i, d in enumerate(inst):
+        assert d["mesh"] == i % 9
+        assert d["wavelength"] == (660 if i % 2 == 0 else 940)
+        assert 0.30 <= d["spo2_f"] <= 0.70 and 0.90 <= d["spo2_m"] <= 1.00
+        assert 1e6 <= d["n_photons"] <= 1e8
+        assert d["first"] == first
+        first += d["n_photons"]
+        nm = np.asarray(d["nmuasg"], np.float32).reshape(-1, 4)
+        assert nm.shape[0] == 6 and np.all(nm[1:, 1] > 0) and np.all(nm[1:, 2] > 0)
+    for w in spec.meshes[1:]:
+        S = shells(np.asarray(w.tri), 12)
+        assert inside_radially(S[4].reshape(-1, 3), S[3], 1.0), "a variant's head crosses the uterine wall"
