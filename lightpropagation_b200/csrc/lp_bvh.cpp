@@ -1,14 +1,15 @@
 // lp_bvh.cpp -- binned-SAH BVH build on the host (see lp_bvh.hpp for the layout).
 //
 // The primitives (box, centroid, original index) are stored contiguously and partitioned
-// in place, so every pass over a node reads memory in order.  The nodes above a size
-// threshold are split on the calling thread; the subtrees below them are independent
-// ranges of the primitive array and are built on worker threads, then appended in a
-// fixed order.  The tree is therefore the same for any thread count.
+// in place, so every pass over a node reads memory in order.  The top levels of the tree
+// are built by a parallel recursion (the two children of a node cover disjoint ranges of
+// the primitive array, so one is built on a new thread) and the largest nodes bin their
+// primitives on several threads.  Every split is decided as in a serial build and the
+// nodes are renumbered breadth-first at the end, so the tree is the same for any thread
+// count.
 #include "lp_bvh.hpp"
 
 #include <algorithm>
-#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -202,17 +203,12 @@ bool split_node(Prim *pr, BNode &nd, int leaf_target, int64_t &mid, int n_thread
 }
 
 // Builds the subtree rooted at nodes[root] (first/count set), appending its nodes.
-void build_from(Prim *pr, std::vector<BNode> &nodes, int32_t root, int leaf_target, int64_t stop_below,
-                std::vector<int32_t> *deferred, int n_threads)
+void build_from(Prim *pr, std::vector<BNode> &nodes, int32_t root, int leaf_target, int n_threads)
 {
     std::vector<int32_t> work{root};
     while (!work.empty()) {
         const int32_t ni = work.back();
         work.pop_back();
-        if (deferred && nodes[ni].count <= stop_below) {
-            deferred->push_back(ni);
-            continue;
-        }
         BNode nd = nodes[ni];
         int64_t mid = 0;
         if (!split_node(pr, nd, leaf_target, mid, n_threads)) {
@@ -232,6 +228,58 @@ void build_from(Prim *pr, std::vector<BNode> &nodes, int32_t root, int leaf_targ
         work.push_back(nd.child[1]);
         work.push_back(nd.child[0]);
     }
+}
+
+constexpr int64_t kParallelGrain = 4096;   // smaller subtrees are built where they are
+
+// Builds the subtree over primitives [first, first + count) into `nodes` and returns its
+// root's index.  While par_depth > 0 and the node is large, its right child is built on a
+// new thread into a vector of its own, appended afterwards with shifted indices; the
+// left child is built on this thread.  Every split is the one the serial build makes
+// (split_node on the same primitive range), so the tree is the same.
+int32_t build_par(Prim *pr, std::vector<BNode> &nodes, int64_t first, int64_t count, int leaf_target,
+                  int par_depth, int bin_threads)
+{
+    const int32_t root = (int32_t)nodes.size();
+    nodes.push_back(BNode());
+    nodes[root].first = first;
+    nodes[root].count = count;
+    if (par_depth <= 0 || count < kParallelGrain) {
+        build_from(pr, nodes, root, leaf_target, bin_threads);
+        return root;
+    }
+    BNode nd = nodes[root];
+    int64_t mid = 0;
+    if (!split_node(pr, nd, leaf_target, mid, bin_threads)) {
+        nodes[root] = nd;
+        return root;
+    }
+    const int sub_bins = std::max(1, bin_threads / 2);
+    std::vector<BNode> right;
+    std::thread th;
+    bool threaded = false;
+    try {
+        th = std::thread([&]() {
+            build_par(pr, right, mid, first + count - mid, leaf_target, par_depth - 1, sub_bins);
+        });
+        threaded = true;
+    } catch (const std::exception &) {
+        // no thread to be had: the right child is built here after the left
+    }
+    nd.child[0] = build_par(pr, nodes, first, mid - first, leaf_target, par_depth - 1, sub_bins);
+    if (threaded)
+        th.join();
+    else
+        build_par(pr, right, mid, first + count - mid, leaf_target, par_depth - 1, sub_bins);
+    const int32_t base = (int32_t)nodes.size();
+    for (BNode b : right) {
+        for (int c = 0; c < 2; ++c)
+            if (b.child[c] >= 0) b.child[c] += base;
+        nodes.push_back(b);
+    }
+    nd.child[1] = base;   // the right subtree's root is its vector's first node
+    nodes[root] = nd;
+    return root;
 }
 
 }  // namespace
@@ -265,50 +313,15 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
 
     std::vector<BNode> nodes;
     nodes.reserve((size_t)(2 * n / std::max(1, leaf_target) + 4));
-    nodes.push_back(BNode());
-    nodes[0].first = 0;
-    nodes[0].count = n;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int n_threads = (int)std::min(hw, 16u);
     if (n < 32768 || n_threads == 1) {
-        build_from(pr.data(), nodes, 0, leaf_target, 0, nullptr, 1);
+        build_par(pr.data(), nodes, 0, n, leaf_target, 0, 1);
     } else {
-        // split the large nodes here; defer the subtrees below the grain to the workers
-        const int64_t grain = std::max<int64_t>(4096, n / (8 * n_threads));
-        std::vector<int32_t> roots;
-        build_from(pr.data(), nodes, 0, leaf_target, grain, &roots, n_threads);
-        std::vector<std::vector<BNode>> sub(roots.size());
-        std::atomic<size_t> next{0};
-        auto worker = [&]() {
-            for (size_t t; (t = next.fetch_add(1)) < roots.size();) {
-                std::vector<BNode> &L = sub[t];
-                L.push_back(nodes[roots[t]]);
-                build_from(pr.data(), L, 0, leaf_target, 0, nullptr, 1);
-            }
-        };
-        std::vector<std::thread> pool;
-        const int nw = (int)std::min<size_t>((size_t)n_threads, roots.size());
-        for (int k = 1; k < nw; ++k) {
-            try {
-                pool.emplace_back(worker);
-            } catch (const std::exception &) {
-                break;   // the threads started so far and this one share the subtrees
-            }
-        }
-        worker();
-        for (std::thread &th : pool) th.join();
-        // append each subtree; its local node 0 replaces the deferred node
-        for (size_t t = 0; t < roots.size(); ++t) {
-            const std::vector<BNode> &L = sub[t];
-            const int32_t base = (int32_t)nodes.size() - 1;
-            auto remap = [&](BNode b) {
-                for (int c = 0; c < 2; ++c)
-                    if (b.child[c] >= 0) b.child[c] += base;
-                return b;
-            };
-            nodes[roots[t]] = remap(L[0]);
-            for (size_t k = 1; k < L.size(); ++k) nodes.push_back(remap(L[k]));
-        }
+        // enough levels of threads for about four subtrees per hardware thread
+        int par_depth = 0;
+        while ((1 << par_depth) < 4 * n_threads) ++par_depth;
+        build_par(pr.data(), nodes, 0, n, leaf_target, par_depth, n_threads);
     }
 
     // A root that is a leaf gets a synthetic internal parent whose two children are
