@@ -3,12 +3,13 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-A step is one pass of the hot path over one batch per case: ``--photons`` photons
-of each case traced through the mesh, tallies zeroed before and complete after.
-The default workload is the curved-mesh abdomen (202,500 triangles, fibre source,
-six ring detectors) at 660 nm and at 940 nm, so a step is two launches on one
-mesh with the media table switched between them; ``--workload plain_slab`` is the
-small 3-layer slab.  Photons are sharded by index range across ranks (weak
+A step is one pass of the hot path over one batch: ``--photons`` photons (1e8 by
+default for the abdomen, the workload's own count) traced through the mesh in one
+launch, tallies zeroed before and complete after.  The default workload is the
+curved-mesh abdomen (202,500 triangles, fibre source, six ring detectors) at 660 nm
+and at 940 nm: steps alternate between the two optical-property tables on one mesh,
+so a job of K steps traces K/2 batches at each wavelength.  ``--workload plain_slab``
+is the small 3-layer slab.  Photons are sharded by index range across ranks (weak
 scaling: every rank traces the same number of photons per step); the integer
 tallies are summed over ranks with one NCCL all-reduce per launch, inside the
 timed region.
@@ -23,7 +24,12 @@ e2e    the same metric through the public API with host buffers: every step sets
        runs, and copies all tallies back to the host.
 roofline  FP32 issue bound: algorithmic FLOPs per photon
        F = 64*E_s + 48*E_b + 40*E_q (scatter events, boundary events, queries per
-       photon, counted by the kernel) over the measured FP32 FMA peak of the device.
+       photon, counted by the kernel) over the measured FP32 FMA peak of the device;
+       beside it the L2-atomic fraction: absorption and exit deposits per second over
+       the measured rate of 64-bit atomic adds to an L2-resident buffer.
+config1_slab  the like-for-like comparison: the 3-layer slab (config 1: pencil beam,
+       reference behaviours on, 1e6 photons) on the GPU and through the reference's
+       own kernel source on the host cores, the same physics on both sides.
 cpu_baseline / --impl reference  the reference kernel source compiled for the CPU
        (oracle/_ref/libclref.so) on all host cores, plus the launcher's host binning,
        on a bounded sample of the same workload.
@@ -57,13 +63,13 @@ def env_int(k, d):
 
 
 def load_cases(name, photons):
-    """The workloads one step traces, in order.  ``curved_abdomen`` (the default) is the
+    """The workloads the steps trace, in turn.  ``curved_abdomen`` (the default) is the
     curved-mesh abdomen at 660 nm and at 940 nm: one mesh, two optical-property tables,
-    a batch of photons at each wavelength per step."""
+    1e8 photons per launch."""
     import dataclasses
     from lightpropagation_b200 import workloads
     if name == "curved_abdomen":
-        w = workloads.curved_abdomen(wavelength=660)
+        w = workloads.curved_abdomen(wavelength=660, n_photons=100_000_000)
         nm940 = np.array(workloads.ABDOMEN_MEDIA[940], np.float32)
         cases = [w, dataclasses.replace(w, nmuasg=nm940, name=w.name.replace("660nm", "940nm"))]
     else:
@@ -72,6 +78,17 @@ def load_cases(name, photons):
         if photons:
             c.n_photons = int(photons)
     return cases
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def ring_rse(det, n):
@@ -239,6 +256,9 @@ def workload_label(args, cases):
 
 
 def reference_arm(args, cases):
+    """The reference's own CPU implementation of the path on all host cores: each step a
+    bounded sample of the step's case (cases alternate as in our arm), plus the
+    like-for-like config-1 slab figure."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
@@ -247,26 +267,38 @@ def reference_arm(args, cases):
     if L is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
-    n = reference_sample_size(cases, threads, 6.0)       # a bounded sample, a few seconds per step
-    for _ in range(args.warmup):
-        reference_sample(cases, max(threads, n // 8), threads)
+    n = reference_sample_size(cases, threads, 3.0 * len(cases))   # a bounded sample, a few seconds per step
+    for i in range(args.warmup):
+        reference_sample([cases[i % len(cases)]], max(threads, n // 8), threads)
     tot_t, tot_n = 0.0, 0
-    for _ in range(args.steps):
-        t, k = reference_sample(cases, n, threads)
+    for i in range(args.steps):
+        t, k = reference_sample([cases[i % len(cases)]], n, threads)
         tot_t += t
         tot_n += k
     v = tot_n / tot_t
     label = workload_label(args, cases)
+    slab = None
+    if args.workload == "curved_abdomen" and not args.no_slab:
+        from lightpropagation_b200 import workloads
+        ws = workloads.plain_slab()
+        m = reference_sample_size([ws], threads, 10.0)
+        dt, k = reference_sample([ws], m, threads)
+        slab = {"workload": ws.name, "reference_photons_per_s": k / dt,
+                "reference_sample": f"{k} photons on {threads} threads",
+                "same_physics": "pencil beam, reference behaviours Q3/Q4/Q10 on, on both sides"}
     line = {"metric": METRIC, "value": v, "unit": "photons/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": label, "photons_per_step": n * len(cases), "triangles": int(cases[0].n_tri),
+            "config": {"workload": label, "photons_per_step_per_gpu": n, "photons_per_launch": n,
+                       "triangles": int(cases[0].n_tri), "steps_alternate": [c.name for c in cases],
                        "parallelism": f"{threads} host threads"},
-            "cpu_baseline": {"value": v, "unit": "photons/s", "cores": threads, "kind": "reference",
-                             "sample": f"{n} photons of each of {len(cases)} case(s) per step of {label}: the "
-                                       f"reference kernel source compiled for the CPU (oracle/_ref, pencil beam "
-                                       f"source, brute-force triangle search) + ExecKernel's host binning"},
-            "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": v, "unit": "photons/s", "cores": threads, "cpu_model": cpu_model(),
+                             "kind": "reference",
+                             "sample": f"{n} photons per step of {label}: the reference kernel source compiled for "
+                                       f"the CPU (oracle/_ref; a pencil beam, its only source; brute-force "
+                                       f"triangle search) + ExecKernel's host binning"},
+            "e2e": {"value": v, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config1_slab": slab}
     print(json.dumps(line))
     return 0
 
@@ -356,6 +388,59 @@ def batched_section(args, local):
     return out
 
 
+def deposits_per_photon(c, n):
+    """Fixed-point atomic deposits per photon the transport makes (the algorithmic count):
+    per scatter event the r-z cell's absorbed weight and absorbed weight over mua and the
+    voxel, less those outside their grids; per photon its exit record's image bins."""
+    es = c["scatter"]
+    return (2.0 * (es - c["rz_drop"]) + (es - c["vox_drop"])) / n + 10.0
+
+
+def slab_section(args, local, peak):
+    """Config 1 on both sides with the same physics: the 3-layer slab, a pencil beam and
+    the reference behaviours on, 1e6 photons per launch.  GPU: device time of 5 launches
+    and e2e through the public API; reference: its kernel source on all host cores."""
+    from lightpropagation_b200 import Simulation, workloads
+    w = workloads.plain_slab()
+    n = w.n_photons
+    sim = Simulation(local)
+    w.apply(sim, seed=0x4C50)
+    for i in range(3):
+        sim.zero()
+        sim.run(n, i * n)
+    ms = []
+    for i in range(5):
+        sim.zero()
+        sim.run(n, (3 + i) * n)
+        ms.append(sim.kernel_ms())
+    t0 = time.perf_counter()
+    for i in range(3):
+        w.apply(sim, seed=0x4C50 + 7 + i)
+        sim.zero()
+        sim.run(n, i * n)
+        sim.tallies()
+    e2e = 3 * n / (time.perf_counter() - t0)
+    cnt = sim.tallies()["counters"]
+    sim.close()
+    out = {"workload": w.name, "photons_per_launch": n, "gpu_photons_per_s": n / (statistics.mean(ms) * 1e-3),
+           "gpu_e2e_photons_per_s": e2e, "gpu_events_per_photon": {"scatter": cnt["scatter"] / n,
+                                                                  "boundary": cnt["boundary"] / n}}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        L, why = reference_lib()
+        if L is None:
+            out["reference_unavailable"] = why
+        else:
+            m = reference_sample_size([w], threads, 10.0)
+            dt, k = reference_sample([w], m, threads)
+            out["reference_photons_per_s"] = k / dt
+            out["reference_sample"] = f"{k} photons on {threads} threads ({cpu_model()})"
+            out["gpu_vs_reference"] = out["gpu_photons_per_s"] / out["reference_photons_per_s"]
+            out["gpu_e2e_vs_reference"] = e2e / out["reference_photons_per_s"]
+    out["same_physics"] = "pencil beam, reference behaviours Q3/Q4/Q10 on, on both sides"
+    return out
+
+
 def ours_arm(args, cases):
     import torch
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -367,7 +452,7 @@ def ours_arm(args, cases):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     from lightpropagation_b200 import Simulation, sharding
-    from lightpropagation_b200.propagation import fp32_peak_tflops
+    from lightpropagation_b200.propagation import fp32_peak_tflops, l2_atomic_peak
     w, ncase = cases[0], len(cases)
     n = w.n_photons
     sim = Simulation(local)
@@ -379,31 +464,29 @@ def ours_arm(args, cases):
         red = sharding.device_tally_tensors(sim, local)
 
     kernel_ms = []          # per timed launch: (case index, device ms)
+    last = {}               # each case's tallies after its last timed launch
 
-    def step(i, keep=None):
-        """One step: a batch of n photons of every case.  Returns device ms (kernels +
-        all-reduce).  `keep` collects each case's tallies after its batch."""
-        ms = 0.0
-        for j, c in enumerate(cases):
-            if ncase > 1:
-                sim.set_media(c.nmuasg)
-            sim.zero()
-            first, count = sharding.photon_range(n * world, rank, world, (i * ncase + j) * n * world)
-            sim.run(count, first)
-            k = sim.kernel_ms()
-            ms += k
-            if keep is not None:
-                kernel_ms.append((j, k))
-            if dist is not None:
-                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                ev0.record()
-                sharding.allreduce_flat(red)
-                ev1.record()
-                ev1.synchronize()
-                ms += ev0.elapsed_time(ev1)
-            if keep is not None and keep.get("last"):
-                keep[j] = sim.tallies()
-        return ms
+    def step(i, timed=False):
+        """Step i: one launch of n photons (per rank) of case i % ncase.  Returns the
+        device ms of the launch plus the all-reduce."""
+        j = i % ncase
+        c = cases[j]
+        if ncase > 1:
+            sim.set_media(c.nmuasg)
+        sim.zero()
+        first, count = sharding.photon_range(n * world, rank, world, i * n * world)
+        sim.run(count, first)
+        ms = sim.kernel_ms()
+        if timed:
+            kernel_ms.append((j, ms))
+        if dist is not None:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            sharding.allreduce_flat(red)
+            ev1.record()
+            ev1.synchronize()
+            ms += ev0.elapsed_time(ev1)
+        return ms, j
 
     for i in range(args.warmup):
         step(i)
@@ -411,6 +494,7 @@ def ours_arm(args, cases):
     # 252 MB block allocated first placed them where the transport kernel ran 15% slower
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
     peak = fp32_peak_tflops(local)
+    atom_peak = l2_atomic_peak(local)
     clocks = ClockSampler(local)
     clocks.start()
     if dist is not None:
@@ -418,12 +502,13 @@ def ours_arm(args, cases):
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
     dev_ms = 0.0
-    last = {}
     for i in range(args.steps):
         flush.fill_(float(i))           # rewrite a 2x-L2 buffer between timed steps
         torch.cuda.synchronize()
-        last["last"] = i == args.steps - 1
-        dev_ms += step(args.warmup + i, keep=last)
+        ms, j = step(args.warmup + i, timed=True)
+        dev_ms += ms
+        if i >= args.steps - ncase:
+            last[j] = sim.tallies()     # after the launch's timing; not part of dev_ms
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -435,7 +520,7 @@ def ours_arm(args, cases):
         t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
-    total_photons = n * ncase * world * args.steps
+    total_photons = n * world * args.steps
     value = total_photons / (t_max * 1e-3)
 
     # gradient cost: one differentiated launch per case (adjoint sums of d(ring signal) /
@@ -444,6 +529,9 @@ def ours_arm(args, cases):
     if rank == 0 and not args.no_gradient and sim._rings.shape[0] and cases[0].nmuasg.shape[0] <= 8:
         grad_ms, plain_ms = 0.0, 0.0
         for j, c in enumerate(cases):
+            ms_j = [k for jj, k in kernel_ms if jj == j]
+            if not ms_j:
+                continue
             if ncase > 1:
                 sim.set_media(c.nmuasg)
             sim.set_gradient(True)
@@ -452,42 +540,40 @@ def ours_arm(args, cases):
             sim.run(n, 10 ** 12 + j * n)
             grad_ms += sim.kernel_ms()
             sim.set_gradient(False)
-            ms_j = [k for jj, k in kernel_ms if jj == j]
             plain_ms += sum(ms_j) / len(ms_j)
         gradient = {"cost_vs_forward": grad_ms / plain_ms, "grad_launch_ms": grad_ms / ncase,
                     "forward_launch_ms": plain_ms / ncase,
                     "derivatives": int(sim._rings.shape[0] * (cases[0].nmuasg.shape[0] - 1) * 2 * ncase),
                     "what": "one launch per case giving d(ring signal)/d(mua, mus) of every region and ring"}
 
-    # e2e through the public API with host buffers, on the long-lived context of the
-    # timed steps (as the reference's CalculatePropagation object is long-lived): every
-    # step sets the mesh (BVH build, then upload and cell-grid build at the next run) and
-    # the other inputs from host arrays, then for each case sets its media, runs and
-    # copies all tallies back.  Creating and releasing a context stays outside: the
+    # e2e through the public API with host buffers, one step per timed step, on the
+    # long-lived context of the timed steps (as the reference's CalculatePropagation object
+    # is long-lived): every step sets the mesh (BVH build, then upload and cell-grid build
+    # at the next run) and the other inputs from host arrays, sets the step's media, runs
+    # and copies all tallies back.  Creating and releasing a context stays outside: the
     # release of a context's buffers took 0.005-2 s on this driver, and the same launch
     # ran up to 30 % slower in a context whose buffers the driver placed after other
-    # large allocations.  transport_ms_per_step is the device time of the step's launches.
+    # large allocations.  transport_ms_per_step is the device time of the step's launch.
     e2e_v = h2d = d2h = e2e_dev_ms = None
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = args.steps
     if rank == 0 or world > 1:
-        e2e_t, e2e_dev_ms = 0.0, 0.0
+        e2e_t, e2e_dev_ms, h2d, d2h = 0.0, 0.0, 0, 0
         for i in range(e2e_steps):
+            c = cases[i % ncase]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            h2d = d2h = 0
-            w.apply(sim, seed=0x4C50 + 1 + i)
-            for j, c in enumerate(cases):
-                if ncase > 1:
-                    sim.set_media(c.nmuasg)
-                sim.zero()
-                sim.run(n, (rank * ncase + j) * n)
-                h2d += sim.stats()["h2d_bytes"]
-                sim.tallies()
-                d2h += sim.stats()["d2h_bytes"]
-                e2e_dev_ms += sim.kernel_ms()
+            c.apply(sim, seed=0x4C50 + 1 + i)
+            sim.zero()
+            sim.run(n, (rank * e2e_steps + i) * n)
+            h2d += sim.stats()["h2d_bytes"]
+            sim.tallies()
+            d2h += sim.stats()["d2h_bytes"]
+            e2e_dev_ms += sim.kernel_ms()
             e2e_t += time.perf_counter() - t0
-        e2e_v = n * ncase * world * e2e_steps / e2e_t
+        e2e_v = n * world * e2e_steps / e2e_t
         e2e_dev_ms /= e2e_steps
+        h2d //= e2e_steps
+        d2h //= e2e_steps
     if dist is None:
         # the batched section's contexts are allocated after this one is released
         sim.close()
@@ -506,36 +592,54 @@ def ours_arm(args, cases):
 
     # roofline of the transport kernel (counters are global after the all-reduce)
     per_launch_photons = n * world
-    flops, launch_ms, events = 0.0, 0.0, {}
+    flops, launch_ms, events, deposits = 0.0, 0.0, {}, 0.0
     rse = {}
     for j, c in enumerate(cases):
+        if j not in last:
+            continue
         cnt = last[j]["counters"]
         F, es, eb, eq = fp32_flops_per_photon(cnt, per_launch_photons)
         ms_j = [k for jj, k in kernel_ms if jj == j]
         flops += F * n * len(ms_j)
+        deposits += deposits_per_photon(cnt, per_launch_photons) * n * len(ms_j)
         launch_ms += sum(ms_j)
         events[c.name] = {"flops_per_photon": F, "scatter": es, "boundary": eb, "query": eq,
                           "query_executed": cnt["query"] / per_launch_photons,
-                          "query_skipped_by_safety_grid": cnt["safe_skip"] / per_launch_photons,
-                          "avg_launch_ms": sum(ms_j) / len(ms_j)}
+                          "query_skipped_by_safety_bounds": cnt["safe_skip"] / per_launch_photons,
+                          "bvh_queries": cnt["bvh_query"] / per_launch_photons,
+                          "deposits_per_photon": deposits_per_photon(cnt, per_launch_photons),
+                          "avg_launch_ms": sum(ms_j) / len(ms_j), "launches": len(ms_j)}
         det = last[j]["det"]
         if det.shape[0]:
             r = ring_rse(det, per_launch_photons)
-            rse[c.name] = {"ring_rse": [float(x) for x in r],
+            k = sum(1 for jj, _ in kernel_ms if jj == j) * per_launch_photons
+            rse[c.name] = {"ring_rse_per_launch": [float(x) for x in r],
+                           "ring_rse_over_the_job": [float(x) * float(np.sqrt(per_launch_photons / k)) for x in r],
+                           "job_photons": int(k),
                            "photons_for_1pct_rse_at_farthest_ring": float(per_launch_photons * (r[-1] / 0.01) ** 2)}
     achieved = flops / (launch_ms * 1e-3) / 1e12
+    atom_rate = deposits / (launch_ms * 1e-3)
     traffic, traffic_photons = traffic_of(args.workload)
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None,
-            "traffic": traffic,
+            "traffic": (traffic * n / traffic_photons) if traffic is not None else None,
             "traffic_note": (f"dram__bytes_read.sum + dram__bytes_write.sum of one {traffic_photons}-photon 660 nm "
-                             f"launch of this workload (ncu, profiles/)") if traffic is not None else None,
+                             f"launch of this workload (ncu, profiles/), scaled to {n} photons")
+            if traffic is not None else None,
             "peak_source": "FP32 FMA peak measured in-run by lp_fp32_peak (MEASURED_PEAKS.json has no FP32 figure)",
+            "l2_atomics": {"achieved_per_s": atom_rate, "peak_per_s": atom_peak,
+                           "frac": atom_rate / atom_peak if atom_peak else None,
+                           "what": "64-bit fixed-point deposits (r-z, voxel, exit bins) per second over the rate "
+                                   "lp_l2_atomic_peak measures in-run"},
             "events_per_photon": events}
 
     batched = None
     if world == 1 and args.batch_instances > 0:
         batched = batched_section(args, local)
+
+    slab = None
+    if world == 1 and args.workload == "curved_abdomen" and not args.no_slab:
+        slab = slab_section(args, local, peak)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -543,7 +647,8 @@ def ours_arm(args, cases):
             threads = os.cpu_count() or 1
             m = reference_sample_size(cases, threads, 12.0)
             dt, k = reference_sample(cases, m, threads)
-            cpu = {"value": k / dt, "unit": "photons/s", "cores": threads, "kind": "reference",
+            cpu = {"value": k / dt, "unit": "photons/s", "cores": threads, "cpu_model": cpu_model(),
+                   "kind": "reference",
                    "sample": f"{m} photons of each case of {workload_label(args, cases)}: the reference kernel "
                              f"source compiled for the CPU (oracle/_ref, pencil beam source, brute-force triangle "
                              f"search) on {threads} threads + ExecKernel's host binning"}
@@ -553,17 +658,18 @@ def ours_arm(args, cases):
     line = {"metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_label(args, cases), "photons_per_step_per_gpu": n * ncase,
+            "config": {"workload": workload_label(args, cases), "photons_per_step_per_gpu": n,
                        "photons_per_launch": n, "triangles": int(w.n_tri),
+                       "steps_alternate": [c.name for c in cases],
                        "parallelism": f"photon ranges x{world}" + (" + NCCL all-reduce of tallies" if world > 1 else ""),
                        "l2": "2x L2 buffer rewritten between timed steps",
                        "arithmetic": "fast (FMA contraction, MCML direction cosines)",
                        "grid": st["grid"], "block": st["block"], "bvh_nodes": st["n_nodes"],
                        "bvh_nodes_in_smem": st["nodes_smem"], "tris_in_smem": st["tris_smem"]},
-            "wall_s": wall, "clocks": clk, "gpu_launches": args.steps * ncase,
+            "wall_s": wall, "clocks": clk, "gpu_launches": args.steps,
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "transport_ms_per_step": e2e_dev_ms},
-            "detector_error": rse, "gradient": gradient, "batched": batched,
+                    "transport_ms_per_step": e2e_dev_ms, "steps": e2e_steps},
+            "detector_error": rse, "gradient": gradient, "batched": batched, "config1_slab": slab,
             "roofline": roof, "cpu_baseline": cpu}
     print(json.dumps(line))
     if sim is not None:
@@ -580,9 +686,10 @@ def main():
     ap.add_argument("--workload", default="curved_abdomen",
                     help="curved_abdomen (660 + 940 nm per step), plain_slab, or another named workload")
     ap.add_argument("--photons", type=int, default=0,
-                    help="photons per launch per GPU (default: the workload's, 1e7 for the abdomen)")
+                    help="photons per launch per GPU (default: the workload's, 1e8 for the abdomen)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient-cost launches")
+    ap.add_argument("--no-slab", action="store_true", help="skip the like-for-like config-1 slab section")
     ap.add_argument("--batch-instances", type=int, default=512, help="instances of the plain-vs-batched "
                     "comparison (0 skips it)")
     ap.add_argument("--batch-min", type=float, default=1e4, help="smallest instance photon budget")

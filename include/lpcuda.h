@@ -49,6 +49,8 @@ extern "C" {
 enum {
     LP_C_SCATTER = 0, LP_C_BOUNDARY, LP_C_QUERY, LP_C_ROULETTE, LP_C_MISS, LP_C_CAPPED,
     LP_C_RZ_DROP, LP_C_VOX_DROP, LP_C_PHOTONS, LP_C_DRAWS, LP_C_SAFE_SKIP, LP_C_BVH_QUERY,
+    LP_C_BAD_INPUT,   /* lp_run_noalloc: triangles whose region ids failed the device-side check */
+    LP_C_BOUNDS,      /* bounds-checked build (liblpcuda_debug.so): accesses skipped as out of range */
     LP_NCOUNTERS = 16
 };
 
@@ -218,6 +220,18 @@ int lp_set_smem_budget(lp_ctx *ctx, int32_t bytes);
  * (0: every query that the safety bound does not skip descends the BVH).  Results are
  * identical either way; lp_query_triangles follows the same setting. */
 int lp_set_cell_lists(lp_ctx *ctx, int enable);
+/* Margin of the cell lists, in cells (default 0.5; 0 to 4): each cell lists the
+ * triangles that touch the cell widened by this margin on every side.  A wider margin
+ * lets more short-step queries be answered from one cell's list and gives larger
+ * distance bounds from the planes of the listed triangles, at the cost of longer lists.
+ * Results do not depend on it.  No reference counterpart. */
+int lp_set_cell_margin(lp_ctx *ctx, float cells);
+/* Warp-aggregated absorption tallies (no reference counterpart; the reference's r-z
+ * tally is a racy read-modify-write, MCLightPropagation.cl:254-271): enable = 1 makes
+ * the lanes of a warp that deposit into the same r-z cell or voxel in the same step sum
+ * their fixed-point values (__match_any_sync + redux.sync) so that one lane issues the
+ * atomic add.  Integer sums: the tallies are identical either way. */
+int lp_set_tally_aggregation(lp_ctx *ctx, int enable);
 /* Per-photon step cap (watchdog); photons that reach it are stopped and counted. */
 int lp_set_max_steps(lp_ctx *ctx, int64_t max_steps);
 /* Keep the per-photon float8 exit records of the next runs (RecordFSTxy,
@@ -240,6 +254,19 @@ int lp_get_geometry(lp_ctx *ctx, lp_geometry *out);
 /* Copy the tallies to host memory owned by ctx (GetSFTImage / GetRTdImage /
  * GetArzImage / GetPhirzImage, CalculatePropagation.cpp:897-1056). */
 int lp_get_tallies(lp_ctx *ctx, lp_tallies *out);
+/* Checkpoint and resume (the reference carries only its ran3 table from launch to
+ * launch, CalculatePropagation.cpp:1213-1215; with Philox a photon's random numbers
+ * depend on the seed and its id alone, so a checkpoint is the seed, the next photon id
+ * and the integer tallies).  lp_set_tallies replaces the context's tallies and counters
+ * with host values in the lp_tallies layout that lp_get_tallies returns for the same
+ * tally grid (sizes n_vox, n_rbins, n_region, n_det must match).  Photons [0, k) traced,
+ * saved, and resumed in another context by lp_set_tallies + lp_run(ctx, k, n - k) give
+ * the tallies of one run of [0, n) bit for bit. */
+int lp_set_tallies(lp_ctx *ctx, const lp_tallies *in);
+/* The FP64 differentiation sums of the same checkpoint, n = n_det * n_media * 5 values in
+ * the layout of lp_set_gradient's sums (ring, region, 5 moments). */
+int lp_get_gradient_sums(lp_ctx *ctx, double *out, int64_t n);
+int lp_set_gradient_sums(lp_ctx *ctx, const double *in, int64_t n);
 /* Copy n exit records (8 floats each) to out. */
 int lp_get_exit_records(lp_ctx *ctx, float *out, int64_t n);
 /* Device time of the last lp_run* in milliseconds (PrintTimeSpent, CP.cpp:2063-2070). */
@@ -263,12 +290,24 @@ typedef struct lp_device_tallies {
     uint64_t *sft, *rtd, *rz, *vox, *rbins, *region, *det, *counters;
     int64_t n_sft, n_rtd, n_rz, n_vox, n_rbins, n_region, n_det, n_counters;
     void *stream;            /* the context's cudaStream_t */
+    double *grad;            /* FP64 differentiation sums (lp_get_gradient_sums layout)  */
+    int64_t n_grad;          /* their count; 0 while differentiation is off             */
 } lp_device_tallies;
 int lp_get_device_tallies(lp_ctx *ctx, lp_device_tallies *out);
 
 /* FP32 FMA throughput of the device in TFLOP/s (2 flops per FMA), measured by a
  * dependent-FMA kernel: the roofline denominator of the transport kernel. */
 int lp_fp32_peak(int device, double *tflops);
+
+/* Throughput of 64-bit atomic adds to random slots of an L2-resident 16 MB buffer, in
+ * atomics per second: the denominator of the transport kernel's L2-atomic fraction. */
+int lp_l2_atomic_peak(int device, double *per_s);
+
+/* Test hook (no reference counterpart): the device or page-locked host allocation made
+ * by this library after `after` more successful ones fails as if memory were exhausted
+ * (the call that needed it returns LP_ERR_NOMEM and leaves its context usable); -1
+ * switches the injection off.  Process-wide. */
+int lp_debug_fail_allocation(int64_t after);
 
 /* --- transport without device allocation ------------------------------------- */
 /* No counterpart in the reference.  For callers that must not allocate device memory
@@ -280,7 +319,13 @@ int lp_fp32_peak(int device, double *tflops);
  * the device from the mesh arrays) lives in one static device array of
  * LP_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
  *   - mesh arrays are DEVICE pointers in the reference layouts (tri 9 floats, nrm 3
- *     floats, med 2 ints per triangle); region ids must be < n_media;
+ *     floats, med 2 ints per triangle); region ids must lie in [0, n_media).  They are
+ *     checked on the device: if any is outside, no photon is traced and
+ *     counters[LP_C_BAD_INPUT] holds the number of such triangles (so pass counters to
+ *     see it); lp_set_mesh rejects the same mesh with LP_ERR_INVALID;
+ *   - dimensions must be finite and positive, and every image extent (dimensions /
+ *     det_grid, 90 / det_grid[5]) below 2^20 cells, else LP_ERR_INVALID / LP_ERR_RANGE;
+ *   - photons stop after LP_NOALLOC_MAX_STEPS steps (counted in LP_C_CAPPED);
  *   - nmuasg is a HOST pointer (n, mua, mus, g per region), copied into kernel params;
  *   - sft, rtd, rz, region are DEVICE outputs in the lp_tallies layouts (sizes as
  *     lp_get_geometry reports for the same dimensions and grid); results are ADDED to
@@ -288,11 +333,14 @@ int lp_fp32_peak(int device, double *tflops);
  *   - sizes beyond LP_NOALLOC_MAX_TRI triangles or LP_NOALLOC_MAX_MEDIA regions are
  *     rejected with LP_ERR_RANGE.
  * The call is asynchronous on `stream` (a cudaStream_t, NULL for the default stream).
- * The first call on a device looks up the scratch address; make that first call
- * before any stream capture.  All calls share the one scratch array, so calls that
- * overlap on the GPU race: serialise them on one stream. */
+ * Each call outside stream capture looks up the scratch address on the current device
+ * (after cudaDeviceReset the array may move); a call inside a capture uses the address
+ * an earlier call on that device found, so make the first call on a device before any
+ * stream capture.  All calls share the one scratch array, so calls that overlap on the
+ * GPU race: serialise them on one stream. */
 #define LP_NOALLOC_MAX_TRI 4096
 #define LP_NOALLOC_MAX_MEDIA 64
+#define LP_NOALLOC_MAX_STEPS 100000000   /* per-photon step cap (lp_run's default) */
 #define LP_NOALLOC_SCRATCH_BYTES (384 * 1024)
 typedef struct lp_noalloc_args {
     const float *tri, *nrm;

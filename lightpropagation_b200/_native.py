@@ -17,7 +17,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "ou
 COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL, COMPAT_ALL = 1, 2, 4, 7
 NCOUNTERS = 16
 COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped", "rz_drop",
-                 "vox_drop", "photons", "draws", "safe_skip", "bvh_query"]
+                 "vox_drop", "photons", "draws", "safe_skip", "bvh_query", "bad_input", "bounds"]
 FIX_ONE = float(2 ** 32)
 
 _fp = C.POINTER(C.c_float)
@@ -49,7 +49,8 @@ class Stats(C.Structure):
 class DeviceTallies(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("sft", "rtd", "rz", "vox", "rbins", "region", "det", "counters")] + \
         [(n, C.c_int64) for n in ("n_sft", "n_rtd", "n_rz", "n_vox", "n_rbins", "n_region", "n_det",
-                                  "n_counters")] + [("stream", C.c_void_p)]
+                                  "n_counters")] + [("stream", C.c_void_p), ("grad", C.c_void_p),
+                                                    ("n_grad", C.c_int64)]
 
 
 class NoAllocArgs(C.Structure):
@@ -109,6 +110,8 @@ _SIGS = {
     "lp_set_arithmetic": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_safety_grid": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_set_cell_lists": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_set_cell_margin": ([C.c_void_p, C.c_float], C.c_int),
+    "lp_set_tally_aggregation": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_smem_budget": ([C.c_void_p, C.c_int32], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
@@ -117,6 +120,9 @@ _SIGS = {
     "lp_zero_tallies": ([C.c_void_p], C.c_int),
     "lp_get_geometry": ([C.c_void_p, C.POINTER(Geometry)], C.c_int),
     "lp_get_tallies": ([C.c_void_p, C.POINTER(Tallies)], C.c_int),
+    "lp_set_tallies": ([C.c_void_p, C.POINTER(Tallies)], C.c_int),
+    "lp_get_gradient_sums": ([C.c_void_p, C.POINTER(C.c_double), C.c_int64], C.c_int),
+    "lp_set_gradient_sums": ([C.c_void_p, C.POINTER(C.c_double), C.c_int64], C.c_int),
     "lp_get_exit_records": ([C.c_void_p, _fp, C.c_int64], C.c_int),
     "lp_last_kernel_ms": ([C.c_void_p, _fp], C.c_int),
     "lp_query_triangles": ([C.c_void_p, C.c_int64, _fp, _fp, _ip, _fp, _ip, _fp], C.c_int),
@@ -124,6 +130,8 @@ _SIGS = {
     "lp_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "lp_get_device_tallies": ([C.c_void_p, C.POINTER(DeviceTallies)], C.c_int),
     "lp_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "lp_l2_atomic_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "lp_debug_fail_allocation": ([C.c_int64], C.c_int),
     "lp_run_noalloc": ([C.POINTER(NoAllocArgs), C.c_void_p], C.c_int),
     "lp_batch_config_count": ([], C.c_int),
     "lp_batch_config_info": ([C.c_int32, _ip, _ip, _ip], C.c_int),
@@ -148,13 +156,18 @@ _SIGS = {
 EXPORTED = sorted(_SIGS)
 
 
+DEBUG_LIB_PATH = os.path.join(os.path.dirname(LIB_PATH), "liblpcuda_debug.so")
+
+
 def lib():
-    """Load liblpcuda.so; raises if it has not been built."""
+    """Load liblpcuda.so (or, with LP_DEBUG_LIBRARY=1 in the environment, the bounds-checked
+    build liblpcuda_debug.so); raises if it has not been built."""
     global _lib
     if _lib is None:
-        if not os.path.isfile(LIB_PATH):
-            raise RuntimeError(f"{LIB_PATH} is missing: build it with lightpropagation_b200.build.build()")
-        L = C.CDLL(LIB_PATH)
+        path = DEBUG_LIB_PATH if os.environ.get("LP_DEBUG_LIBRARY") == "1" else LIB_PATH
+        if not os.path.isfile(path):
+            raise RuntimeError(f"{path} is missing: build it with lightpropagation_b200.build.build()")
+        L = C.CDLL(path)
         for name, (args, res) in _SIGS.items():
             f = getattr(L, name)
             f.argtypes = args

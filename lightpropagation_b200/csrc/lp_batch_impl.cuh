@@ -61,6 +61,9 @@ __device__ __forceinline__ void warp_load_slot(WarpSlot &S, const KParams *inst,
         M.s_ta = M.s_tb = M.s_tc = nullptr;
         M.nodes_smem = 0;
         M.tris_smem = 0;
+        M.n_nodes = S.P.n_nodes;
+        M.n_tri = S.P.n_tri;
+        M.dbg = S.P.counters ? S.P.counters + kBoundsCounter : nullptr;
     }
     __syncwarp();
 }

@@ -389,9 +389,22 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
         float Fx = t[3] - t[6], Fy = t[4] - t[7], Fz = t[5] - t[8];
         float ob;
         std::memcpy(&ob, &oi, 4);
+        // plane-distance factors: |(G x E) . F| * inv_n is the distance from a point to the
+        // triangle's plane (G = point - M), and kappa * |G|_1 bounds the rounding of that
+        // product in float (about 9 ulp of |G| |E| |F| / |E x F|, taken 10x larger here);
+        // a degenerate triangle gets 0, 0, so its plane distance reads 0
+        const double ex = Ex, ey = Ey, ez = Ez, fx = Fx, fy = Fy, fz = Fz;
+        const double nx = ey * fz - ez * fy, ny = ez * fx - ex * fz, nz = ex * fy - ey * fx;
+        const double nl = std::sqrt(nx * nx + ny * ny + nz * nz);
+        const double el = std::sqrt(ex * ex + ey * ey + ez * ez), fl = std::sqrt(fx * fx + fy * fy + fz * fz);
+        float inv_n = 0.0f, kappa = 0.0f;
+        if (nl > 1e-30 * (el * fl + 1e-300) && std::isfinite(nl)) {
+            inv_n = (float)((1.0 / nl) * (1.0 - 1e-6));
+            kappa = (float)std::min(1e-5 * el * fl / nl, 1e30);
+        }
         out.tri_a[j] = {t[6], t[7], t[8], Ex};
         out.tri_b[j] = {Ey, Ez, Fx, Fy};
-        out.tri_c[j] = {Fz, ob, 0.0f, 0.0f};
+        out.tri_c[j] = {Fz, ob, inv_n, kappa};
     }
 }
 

@@ -15,7 +15,8 @@
 //               ref < 0 leaf with ~ref = (first << 3) | (count - 1)
 //   tri_a[j]  = (M.x, M.y, M.z, E.x)    triangle j in leaf order, E = K - M
 //   tri_b[j]  = (E.y, E.z, F.x, F.y)    F = L - M
-//   tri_c[j]  = (F.z, original index as int bits, 0, 0)
+//   tri_c[j]  = (F.z, original index as int bits, inv_n, kappa): 1 / |E x F| and the
+//               rounding factor of the plane distance |(G x E) . F| * inv_n (see build_bvh)
 // Boxes are widened by a small absolute margin so that rounding in the ray/box
 // test never culls a triangle the exact test accepts.
 #pragma once

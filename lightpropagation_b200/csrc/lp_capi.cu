@@ -8,12 +8,15 @@
 // device.  No exceptions cross the ABI; errors are int codes plus a message.
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -42,6 +45,7 @@ cudaError_t launch_cell_lists(const KParams &P, int n_tri, float h, float eps, u
 cudaError_t launch_cell_words(int64_t n, const uint16_t *safe, const uint32_t *count, const uint32_t *start, bool lists,
                               uint32_t *word, cudaStream_t s);
 double fma_peak_tflops(int num_sms);
+double red_peak_per_s(int num_sms);
 int block_size();
 }  // namespace lp
 
@@ -52,6 +56,29 @@ namespace {
 
 thread_local std::string g_thread_error;
 
+// An NVTX range over a phase of the host path (mesh build, upload, cell grid, launch,
+// wait, readback), seen by profilers on the context's timeline; the counterpart of the
+// reference's per-launch OpenCL profiling events (CalculatePropagation.cpp:1229, 1544-1548).
+struct Phase {
+    explicit Phase(const char *name) { nvtxRangePushA(name); }
+    ~Phase() { nvtxRangePop(); }
+    Phase(const Phase &) = delete;
+    Phase &operator=(const Phase &) = delete;
+};
+
+// Allocation-failure injection (lp_debug_fail_allocation): the allocation that brings the
+// countdown from 0 to -1 reports cudaErrorMemoryAllocation without allocating.
+std::atomic<int64_t> g_alloc_countdown{-1};
+
+bool injected_alloc_failure()
+{
+    int64_t v = g_alloc_countdown.load();
+    while (v >= 0) {
+        if (g_alloc_countdown.compare_exchange_weak(v, v - 1)) return v == 0;
+    }
+    return false;
+}
+
 template <class T>
 struct DevBuf {
     T *p = nullptr;
@@ -60,6 +87,7 @@ struct DevBuf {
     {
         if (count <= n && p) return cudaSuccess;
         release();
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
         if (e != cudaSuccess) {
             p = nullptr;
@@ -92,6 +120,7 @@ struct HostBuf {
             if (p) cudaFreeHost(p);
             p = nullptr;
             cap = n = 0;
+            if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
             cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&p), count * sizeof(T), cudaHostAllocPortable);
             if (e != cudaSuccess) {
                 p = nullptr;
@@ -219,7 +248,10 @@ struct lp_ctx {
     DevBuf<uint32_t> cell_word;
     DevBuf<int32_t> cell_refs;
     int64_t n_cell_refs = 0;
-    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0;
+    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0, g_step_eps = 0;
+    // lists hold the triangles touching each cell widened by cell_margin cells on every side
+    float cell_margin = 0.5f;
+    bool agg_tallies = false;   // lp_set_tally_aggregation
     int32_t g_n[3] = {0, 0, 0};
     float grid_ms = 0;
     // differentiation (lp_set_gradient / lp_forward / lp_backward)
@@ -252,7 +284,8 @@ int fail(lp_ctx *c, int code, const char *fmt, ...)
 
 int cuda_fail(lp_ctx *c, cudaError_t e, const char *what)
 {
-    return fail(c, LP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return fail(c, e == cudaErrorMemoryAllocation ? LP_ERR_NOMEM : LP_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
 }
 
 #define LP_CUDA(ctx, call)                                   \
@@ -327,6 +360,7 @@ int zero_tallies(lp_ctx *c)
 
 int upload_mesh(lp_ctx *c)
 {
+    Phase phase("lp mesh upload");
     if (!c->mesh_dirty) return LP_OK;
     const lp::Bvh &b = c->bvh;
     const size_t nn = b.node_a.size(), nt = b.tri_a.size();
@@ -509,6 +543,7 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     const bool grid = c->grid_max_cells > 0 && c->cell_word.p && !c->grid_dirty;
     P.cell_word = grid ? c->cell_word.p : nullptr;
     P.cell_refs = (grid && c->cell_lists && c->n_cell_refs > 0) ? c->cell_refs.p : nullptr;
+    P.n_cell_refs = P.cell_refs ? c->n_cell_refs : 0;
     P.g_eps = c->g_eps;
     P.g_ox = c->g_origin[0];
     P.g_oy = c->g_origin[1];
@@ -518,6 +553,10 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.g_nx = c->g_n[0];
     P.g_ny = c->g_n[1];
     P.g_nz = c->g_n[2];
+    P.g_h = c->g_h;
+    P.g_margin = c->cell_margin * c->g_h;
+    P.step_eps = c->g_step_eps;
+    P.agg_tallies = c->agg_tallies ? 1 : 0;
 }
 
 // Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
@@ -530,6 +569,7 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
 //   5. cell_word_kernel: one word per cell (KParams::cell_word).
 int build_safety_grid(lp_ctx *c)
 {
+    Phase phase("lp cell grid build");
     c->grid_dirty = false;
     c->n_cell_refs = 0;
     if (c->grid_max_cells <= 0 || c->n_tri == 0) {
@@ -562,6 +602,9 @@ int build_safety_grid(lp_ctx *c)
     // list margin: far above the rounding of coordinates and of the ray/triangle test's
     // intersection point at this scale, far below any cell size
     c->g_eps = (float)(2e-5 * scale);
+    // rounding of one position update p + s v: under 2 ulp of the largest coordinate per
+    // component; 5e-7 * scale is about 4 ulp (2^-23 = 1.19e-7)
+    c->g_step_eps = (float)(5e-7 * scale);
     for (int a = 0; a < 3; ++a) c->g_origin[a] = (float)(b.lo[a] - h);
     DevBuf<uint16_t> safe;
     DevBuf<float> level[4];   // block distances of the safety grid's levels 1..3
@@ -601,12 +644,14 @@ int build_safety_grid(lp_ctx *c)
         e = lp::launch_safety_grid(P, (float)h, (float)(h * std::sqrt(3.0) / 2.0), eps, (float)(64.0 * h), lv, n_levels,
                                    safe.p, s);
     bool lists = false;
+    // every list holds the triangles that touch its cell widened by the margin plus g_eps
+    const float list_eps = c->cell_margin * c->g_h + c->g_eps;
     if (e == cudaSuccess && c->cell_lists) {
         const int nt = (int)c->bvh.tri_a.size();
         size_t tmp_bytes = 0;
         if ((e = count.ensure((size_t)cells)) == cudaSuccess && (e = start.ensure((size_t)cells)) == cudaSuccess &&
             (e = cudaMemsetAsync(count.p, 0, (size_t)cells * 4, s)) == cudaSuccess &&
-            (e = lp::launch_cell_lists(P, nt, c->g_h, c->g_eps, count.p, nullptr, nullptr, s)) == cudaSuccess &&
+            (e = lp::launch_cell_lists(P, nt, c->g_h, list_eps, count.p, nullptr, nullptr, s)) == cudaSuccess &&
             (e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, count.p, start.p, cells, s)) == cudaSuccess &&
             (e = scan_tmp.ensure(tmp_bytes)) == cudaSuccess &&
             (e = cub::DeviceScan::ExclusiveSum(scan_tmp.p, tmp_bytes, count.p, start.p, cells, s)) == cudaSuccess) {
@@ -619,7 +664,7 @@ int build_safety_grid(lp_ctx *c)
                 if (total > 0 && total <= (int64_t(1) << 28)) {
                     if ((e = c->cell_refs.ensure((size_t)total)) == cudaSuccess &&
                         (e = cudaMemsetAsync(count.p, 0, (size_t)cells * 4, s)) == cudaSuccess &&
-                        (e = lp::launch_cell_lists(P, nt, c->g_h, c->g_eps, count.p, start.p, c->cell_refs.p, s)) ==
+                        (e = lp::launch_cell_lists(P, nt, c->g_h, list_eps, count.p, start.p, c->cell_refs.p, s)) ==
                             cudaSuccess) {
                         lists = true;
                         c->n_cell_refs = total;
@@ -656,6 +701,13 @@ void smem_plan(const lp_ctx *c, int budget, int &nodes_smem, int &tris_smem)
 
 // helpers shared with lp_noalloc.cu
 namespace lp {
+// Held from setting a transport kernel's shared-memory attribute to its launch: the
+// attribute belongs to the kernel, not to a context or a call.
+std::mutex &launch_mutex()
+{
+    static std::mutex m;
+    return m;
+}
 void set_thread_error(const char *msg) { g_thread_error = msg; }
 float rspecular_of(const float *nmuasg, int n_media) { return rspecular(nmuasg, n_media); }
 }  // namespace lp
@@ -713,6 +765,7 @@ void lp_destroy(lp_ctx *c)
 
 int lp_set_mesh(lp_ctx *c, int64_t n_tri, const float *tri, const float *nrm, const int32_t *med)
 {
+    Phase phase("lp BVH build");
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_mesh: ctx is NULL");
     if (n_tri <= 0 || !tri || !nrm || !med) return fail(c, LP_ERR_INVALID, "lp_set_mesh: empty mesh or NULL array");
     if (n_tri > (int64_t(1) << 27)) return fail(c, LP_ERR_RANGE, "lp_set_mesh: %lld triangles > 2^27", (long long)n_tri);
@@ -852,6 +905,24 @@ int lp_set_arithmetic(lp_ctx *c, int exact)
     return LP_OK;
 }
 
+int lp_set_tally_aggregation(lp_ctx *c, int enable)
+{
+    if (!c) return LP_ERR_INVALID;
+    c->agg_tallies = enable != 0;
+    return LP_OK;
+}
+
+int lp_set_cell_margin(lp_ctx *c, float cells)
+{
+    if (!c) return LP_ERR_INVALID;
+    if (!(cells >= 0.0f && cells <= 4.0f)) return fail(c, LP_ERR_INVALID, "lp_set_cell_margin: %g cells", (double)cells);
+    if (cells != c->cell_margin) {
+        c->cell_margin = cells;
+        c->grid_dirty = true;
+    }
+    return LP_OK;
+}
+
 int lp_set_safety_grid(lp_ctx *c, int64_t max_cells)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_safety_grid: ctx is NULL");
@@ -959,6 +1030,7 @@ int lp_set_exit_records(lp_ctx *c, int64_t capacity)
 
 int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
 {
+    Phase phase("lp transport launch");
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_run: ctx is NULL");
     if (n < 0 || first < 0) return fail(c, LP_ERR_INVALID, "lp_run: negative photon range");
     c->h2d_bytes = 0;
@@ -972,6 +1044,9 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
     smem_plan(c, c->smem_budget, nodes_smem, tris_smem);
     const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     int per_sm = 0;
+    // the shared-memory attribute set by the occupancy query is process-wide; the lock
+    // keeps another thread's setting from landing between it and this launch
+    std::lock_guard<std::mutex> launch_lock(lp::launch_mutex());
     if (c->grad_on)
         LP_CUDA(c, c->exact ? lp::transport_occupancy_exact_grad(smem, &per_sm)
                             : lp::transport_occupancy_fast_grad(smem, &per_sm));
@@ -999,6 +1074,7 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
 
 int lp_sync(lp_ctx *c)
 {
+    Phase phase("lp transport wait");
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_sync: ctx is NULL");
     LP_CUDA(c, cudaStreamSynchronize(c->stream));
     if (c->launched) {
@@ -1035,6 +1111,7 @@ int lp_get_geometry(lp_ctx *c, lp_geometry *out)
 
 int lp_get_tallies(lp_ctx *c, lp_tallies *out)
 {
+    Phase phase("lp tally readback");
     if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_tallies: NULL argument");
     if (c->tally_dirty || !c->sft.p) return fail(c, LP_ERR_STATE, "lp_get_tallies: nothing has run");
     const lp_geometry &g = c->geo;
@@ -1071,6 +1148,70 @@ int lp_get_tallies(lp_ctx *c, lp_tallies *out)
     out->n_rbins = c->n_rbins;
     out->n_region = c->n_media;
     out->n_det = (int64_t)c->det_r.size() / 2;
+    return LP_OK;
+}
+
+int lp_set_tallies(lp_ctx *c, const lp_tallies *in)
+{
+    if (!c || !in) return fail(c, LP_ERR_INVALID, "lp_set_tallies: NULL argument");
+    if (!c->have_grid) return fail(c, LP_ERR_STATE, "lp_set_tallies: tally grid not set");
+    const lp_geometry &g = c->geo;
+    const int64_t D = (int64_t)c->det_r.size() / 2;
+    if (in->n_vox != n_vox(c) || in->n_rbins != c->n_rbins || in->n_region != c->n_media || in->n_det != D)
+        return fail(c, LP_ERR_INVALID,
+                    "lp_set_tallies: layout differs from the context's (vox %lld/%lld, rbins %lld/%d, regions "
+                    "%lld/%d, rings %lld/%lld)", (long long)in->n_vox, (long long)n_vox(c), (long long)in->n_rbins,
+                    c->n_rbins, (long long)in->n_region, c->n_media, (long long)in->n_det, (long long)D);
+    if (!in->sft || !in->rtd || !in->rz || !in->region || (in->n_vox && !in->vox) || (in->n_rbins && !in->rbins) ||
+        (D && !in->det))
+        return fail(c, LP_ERR_INVALID, "lp_set_tallies: NULL tally array");
+    LP_CUDA(c, cudaSetDevice(c->device));
+    if (c->tally_dirty) {
+        int r = alloc_tallies(c);
+        if (r) return r;
+        r = zero_tallies(c);
+        if (r) return r;
+        c->tally_dirty = false;
+    }
+    cudaStream_t s = c->stream;
+    LP_CUDA(c, cudaMemcpyAsync(c->sft.p, in->sft, (size_t)g.sft_nx * g.sft_ny * 3 * 8, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->rtd.p, in->rtd, (size_t)g.dimR * g.dimAlpha * 3 * 8, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->rz.p, in->rz, (size_t)g.rz_nr * g.rz_nz * 2 * 8, cudaMemcpyHostToDevice, s));
+    if (in->n_vox) LP_CUDA(c, cudaMemcpyAsync(c->vox.p, in->vox, (size_t)in->n_vox * 8, cudaMemcpyHostToDevice, s));
+    if (in->n_rbins)
+        LP_CUDA(c, cudaMemcpyAsync(c->rbins.p, in->rbins, (size_t)in->n_rbins * 2 * 8, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->region.p, in->region, (size_t)in->n_region * 8, cudaMemcpyHostToDevice, s));
+    if (D) LP_CUDA(c, cudaMemcpyAsync(c->det.p, in->det, (size_t)D * 2 * 8, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaMemcpyAsync(c->counters.p, in->counters, LP_NCOUNTERS * 8, cudaMemcpyHostToDevice, s));
+    LP_CUDA(c, cudaStreamSynchronize(s));
+    return LP_OK;
+}
+
+int lp_get_gradient_sums(lp_ctx *c, double *out, int64_t n)
+{
+    if (!c || !out) return fail(c, LP_ERR_INVALID, "lp_get_gradient_sums: NULL argument");
+    const int64_t want = (int64_t)(c->det_r.size() / 2) * c->n_media * 5;
+    if (n != want) return fail(c, LP_ERR_INVALID, "lp_get_gradient_sums: %lld values, the layout has %lld",
+                               (long long)n, (long long)want);
+    if (!c->grad.p) return fail(c, LP_ERR_STATE, "lp_get_gradient_sums: nothing has run");
+    if (n == 0) return LP_OK;
+    LP_CUDA(c, cudaSetDevice(c->device));
+    LP_CUDA(c, cudaMemcpyAsync(out, c->grad.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    LP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LP_OK;
+}
+
+int lp_set_gradient_sums(lp_ctx *c, const double *in, int64_t n)
+{
+    if (!c || !in) return fail(c, LP_ERR_INVALID, "lp_set_gradient_sums: NULL argument");
+    const int64_t want = (int64_t)(c->det_r.size() / 2) * c->n_media * 5;
+    if (n != want) return fail(c, LP_ERR_INVALID, "lp_set_gradient_sums: %lld values, the layout has %lld",
+                               (long long)n, (long long)want);
+    if (c->tally_dirty || !c->grad.p) return fail(c, LP_ERR_STATE, "lp_set_gradient_sums: set the tallies first");
+    if (n == 0) return LP_OK;
+    LP_CUDA(c, cudaSetDevice(c->device));
+    LP_CUDA(c, cudaMemcpyAsync(c->grad.p, in, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    LP_CUDA(c, cudaStreamSynchronize(c->stream));
     return LP_OK;
 }
 
@@ -1126,6 +1267,8 @@ int lp_get_device_tallies(lp_ctx *c, lp_device_tallies *out)
     out->n_det = (int64_t)c->det_r.size();
     out->n_counters = LP_NCOUNTERS;
     out->stream = (void *)c->stream;
+    out->grad = c->grad.p;
+    out->n_grad = c->grad_on ? (int64_t)(c->det_r.size() / 2) * c->n_media * 5 : 0;
     return LP_OK;
 }
 
@@ -1139,6 +1282,25 @@ int lp_fp32_peak(int device, double *tflops)
     *tflops = lp::fma_peak_tflops(sms);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_fp32_peak");
+    return LP_OK;
+}
+
+int lp_debug_fail_allocation(int64_t after)
+{
+    g_alloc_countdown.store(after < 0 ? -1 : after);
+    return LP_OK;
+}
+
+int lp_l2_atomic_peak(int device, double *per_s)
+{
+    if (!per_s) return fail(nullptr, LP_ERR_INVALID, "lp_l2_atomic_peak: NULL argument");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_l2_atomic_peak");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    *per_s = lp::red_peak_per_s(sms);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "lp_l2_atomic_peak");
     return LP_OK;
 }
 
@@ -1578,6 +1740,7 @@ int lp_batch_autotune(lp_batch *b, int64_t photons, int32_t *best, double *ns_pe
 
 int lp_batch_run(lp_batch *b)
 {
+    Phase phase("lp batch graph launch");
     if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_run: batch is NULL");
     if (b->inst.empty()) return LP_OK;
     LP_BCUDA(b, cudaSetDevice(b->device));

@@ -81,8 +81,14 @@ struct KParams {
     // cell_refs holds BVH-order triangle indices.  Null cell_word: BVH queries only.
     const uint32_t *cell_word;
     const int32_t *cell_refs;   // null: the words carry safety bounds only
+    int64_t n_cell_refs;
     float g_ox, g_oy, g_oz, g_inv_h, g_unit, g_eps;
     int32_t g_nx, g_ny, g_nz;
+    // a cell's list holds every triangle touching the cell widened by g_margin + g_eps on
+    // every side; g_h is the cell edge; step_eps bounds the rounding of one position update
+    float g_margin, g_h, step_eps;
+    // 1: absorption deposits are summed per cell across the warp before the atomic adds
+    int32_t agg_tallies;
     // scratch: photon work counter
     unsigned long long *work;
 };
@@ -95,6 +101,23 @@ struct BatchParams {
     int32_t *frontier;               // lowest instance that may still have unclaimed photons
     int32_t n_inst;
 };
+
+// Bounds checks of the debug build (compiled with -DLP_DEBUG into liblpcuda_debug.so):
+// an index outside its array is counted in the counter slot LP_C_BOUNDS (13) and the
+// access is skipped, so a bad index is reported instead of reading or writing past an
+// allocation.  The release build compiles every check to `true`.
+constexpr int kBoundsCounter = 13;
+__device__ __forceinline__ bool in_range_dbg(unsigned long long *dbg, long long i, long long n)
+{
+    const bool ok = i >= 0 && i < n;
+    if (!ok && dbg) atomicAdd(dbg, 1ull);
+    return ok;
+}
+#ifdef LP_DEBUG
+#define LP_IN_RANGE(dbg, i, n) ::lp::in_range_dbg((dbg), (long long)(i), (long long)(n))
+#else
+#define LP_IN_RANGE(dbg, i, n) true
+#endif
 
 constexpr uint32_t kCellEmpty = 0x80000000u;
 constexpr uint32_t kCellDense = 127u;
@@ -109,6 +132,16 @@ __device__ __forceinline__ uint32_t cell_at(const KParams &P, float px, float py
     const int iz = (int)floorf((pz - P.g_oz) * P.g_inv_h);
     if (ix < 0 || iy < 0 || iz < 0 || ix >= P.g_nx || iy >= P.g_ny || iz >= P.g_nz) return kCellEmpty;
     return __ldg(P.cell_word + ((int64_t)iz * P.g_ny + iy) * P.g_nx + ix);
+}
+
+// Distance from p to the nearest face of the cell containing it (0 outside the grid):
+// the smallest of the fractional cell coordinates and their complements, times h.
+__device__ __forceinline__ float cell_face_distance(const KParams &P, float px, float py, float pz)
+{
+    const float fx = (px - P.g_ox) * P.g_inv_h, fy = (py - P.g_oy) * P.g_inv_h, fz = (pz - P.g_oz) * P.g_inv_h;
+    const float rx = fx - floorf(fx), ry = fy - floorf(fy), rz = fz - floorf(fz);
+    const float d = fminf(fminf(fminf(rx, 1.0f - rx), fminf(ry, 1.0f - ry)), fminf(rz, 1.0f - rz));
+    return fmaxf(d, 0.0f) * P.g_h;
 }
 
 // Conservative distance from p to the nearest triangle (0 near a surface).
@@ -208,11 +241,14 @@ struct MeshView {
     const int4 *s_nd;
     const float4 *s_ta, *s_tb, *s_tc;
     int32_t nodes_smem, tris_smem;
+    int32_t n_nodes, n_tri;          // array sizes for the debug build's bounds checks
+    unsigned long long *dbg;         // its counter of skipped accesses (may be null)
 };
 
 __device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, int ref_tri, float &best,
                                          int &bid)
 {
+    if (!LP_IN_RANGE(M.dbg, j, M.n_tri)) return;
     float4 a, b, c;
     if (j < M.tris_smem) {
         a = M.s_ta[j]; b = M.s_tb[j]; c = M.s_tc[j];
@@ -245,6 +281,47 @@ __device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, i
     }
 }
 
+// test_tri plus a lower bound of the distance from p to the triangle: the distance to
+// its plane, |(G x E) . F| / |E x F|, less a bound of the rounding of that product
+// (tri_c.z = 1 / |E x F|, tri_c.w = the rounding factor per unit |G|, see lp_bvh.hpp).
+// safe is lowered to that bound; the hit test is test_tri's, operation for operation.
+__device__ __forceinline__ void test_tri_safe(const MeshView &M, int j, V3 p, V3 v, int ref_tri, float &best,
+                                              int &bid, float &safe)
+{
+    if (!LP_IN_RANGE(M.dbg, j, M.n_tri)) {
+        safe = 0.0f;
+        return;
+    }
+    float4 a, b, c;
+    if (j < M.tris_smem) {
+        a = M.s_ta[j]; b = M.s_tb[j]; c = M.s_tc[j];
+    } else {
+        a = __ldg(M.ta + j); b = __ldg(M.tb + j); c = __ldg(M.tc + j);
+    }
+    const V3 Mv = v3(a.x, a.y, a.z), E = v3(a.w, b.x, b.y), F = v3(b.z, b.w, c.x);
+    const V3 G = sub3(p, Mv);
+    const V3 GE = cross3(G, E);
+    float t = dot3(GE, F);
+    safe = fminf(safe, fabsf(t) * c.z - c.w * (fabsf(G.x) + fabsf(G.y) + fabsf(G.z)));
+    const int o = __float_as_int(c.y);
+    if (o == ref_tri) return;
+    const V3 VF = cross3(v, F);
+    const float w = dot3(VF, E);
+    float k = dot3(VF, G);
+    float l = dot3(GE, v);
+    const float aw = fabsf(w);
+    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= 0.0f && l >= 0.0f) : (t < 0.0f && k <= 0.0f && l <= 0.0f);
+    if (!sgn || fabsf(k) + fabsf(l) > aw * 1.0001f || fabsf(t) > best * aw * 1.0001f) return;
+    t = t / w;
+    k = k / w;
+    l = l / w;
+    if (t > 0.0f && t < kNoHit && k >= 0.0f && l >= 0.0f && (k + l) < 1.0f &&
+        (t < best || (t == best && o < bid))) {
+        best = t;
+        bid = o;
+    }
+}
+
 // STACK: traversal stack entries; the host only runs a tree whose depth is below it.
 template <int STACK = kStackDepth>
 __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
@@ -262,6 +339,7 @@ __device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int 
     for (;;) {
         float4 a, b, c;
         int4 d;
+        if (!LP_IN_RANGE(M.dbg, node, M.n_nodes)) break;
         if (node < M.nodes_smem) {
             a = M.s_na[node]; b = M.s_nb[node]; c = M.s_nc[node]; d = M.s_nd[node];
         } else {
@@ -346,8 +424,9 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
             for (int x = x0; x <= x1; ++x) {
                 const uint32_t w = __ldg(P.cell_word + ((int64_t)z * ny + y) * nx + x);
                 if (w & kCellEmpty) continue;
-                const uint32_t cnt = (w >> 24) & 127u;
+                uint32_t cnt = (w >> 24) & 127u;
                 if (cnt == kCellDense) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
+                if (!LP_IN_RANGE(M.dbg, (int64_t)(w & 0xffffffu) + cnt - 1, P.n_cell_refs)) cnt = 0;
                 const int32_t *r = P.cell_refs + (w & 0xffffffu);
                 for (uint32_t k = 0; k < cnt; ++k) test_tri(M, __ldg(r + k), p, v, ref_tri, best, bid);
             }
@@ -358,6 +437,39 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
     }
     t_out = best;
     return bid;
+}
+
+// The query answered from the list of p's own cell (word: a list word, not dense),
+// together with a lower bound `safe` of the distance from p to every triangle of the
+// mesh.  The list holds every triangle touching the cell widened by g_margin + g_eps, so
+// an unlisted triangle lies at least g_margin + dface from p (dface: distance from p to
+// the cell's faces), and no segment from p of length <= reach = g_margin + dface - g_eps
+// can reach one.  For listed triangles the bound is their plane distance.  On a
+// triangle (ref_tri >= 0) the bound is 0.  Returns false, with safe still valid, when
+// bound > reach: the list alone does not decide the query then.
+__device__ __forceinline__ bool list_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
+                                           uint32_t word, float &t_out, int &tri_out, float &safe)
+{
+    const float reach = P.g_margin + cell_face_distance(P, p.x, p.y, p.z) - P.g_eps;
+    uint32_t cnt = (word >> 24) & 127u;
+    const int32_t *r = P.cell_refs + (word & 0xffffffu);
+    float best = bound, s = reach;
+    if (!LP_IN_RANGE(M.dbg, (int64_t)(word & 0xffffffu) + cnt - 1, P.n_cell_refs)) {
+        cnt = 0;
+        s = 0.0f;
+    }
+    int bid = 0x7fffffff;
+    for (uint32_t k = 0; k < cnt; ++k) test_tri_safe(M, __ldg(r + k), p, v, ref_tri, best, bid, s);
+    safe = ref_tri >= 0 ? 0.0f : fmaxf(s - P.g_eps, 0.0f);
+    if (!(bound <= reach)) return false;
+    if (bid == 0x7fffffff) {
+        t_out = kNoHit;
+        tri_out = -1;
+    } else {
+        t_out = best;
+        tri_out = bid;
+    }
+    return true;
 }
 
 }  // namespace lp

@@ -28,6 +28,7 @@ cudaError_t launch_transport_exact(const KParams &P, int grid, int smem, cudaStr
 cudaError_t transport_occupancy_exact(int smem, int *blocks_per_sm);
 void set_thread_error(const char *msg);
 float rspecular_of(const float *nmuasg, int n_media);
+std::mutex &launch_mutex();
 }  // namespace lp
 
 namespace {
@@ -38,6 +39,9 @@ constexpr int kMaxLeaves = (LP_NOALLOC_MAX_TRI + kLeafTris - 1) / kLeafTris;
 constexpr int kMaxNodes = kMaxLeaves;
 constexpr size_t OFF_WORK = 0;
 constexpr size_t OFF_CNT = 8;                       // 16 counters -> 136 bytes used
+// set as the work counter when the mesh fails the device-side check: every photon index
+// handed out is then past the range, so the transport kernel traces nothing
+constexpr unsigned long long kRejectAll = 1ull << 62;
 constexpr size_t HEADER = 256;                      // cleared at every call
 constexpr size_t OFF_MEDIA = HEADER;
 constexpr size_t OFF_NODE_A = OFF_MEDIA + LP_NOALLOC_MAX_MEDIA * sizeof(Medium);
@@ -117,8 +121,14 @@ __global__ void __launch_bounds__(256) noalloc_setup_kernel(const float *tri, co
             y = __fdiv_rn(y, l);
             z = __fdiv_rn(z, l);
         }
-        const int inner = min(max(med[2 * (int64_t)j], 0), mp.n - 1);
-        const int outer = min(max(med[2 * (int64_t)j + 1], 0), mp.n - 1);
+        const int in_id = med[2 * (int64_t)j], out_id = med[2 * (int64_t)j + 1];
+        if (in_id < 0 || in_id >= mp.n || out_id < 0 || out_id >= mp.n) {
+            // lp_set_mesh rejects such an id; here the mesh lives in device memory, so the
+            // check is made on the device: the triangle is counted and nothing is traced
+            atomicAdd(reinterpret_cast<unsigned long long *>(s + OFF_CNT) + LP_C_BAD_INPUT, 1ull);
+        }
+        const int inner = min(max(in_id, 0), mp.n - 1);
+        const int outer = min(max(out_id, 0), mp.n - 1);
         at[j] = make_float4(x, y, z, __int_as_float(inner | (outer << 16)));
         for (int k = 0; k < 9; ++k) amax = fmaxf(amax, fabsf(t[k]));
         for (int v = 0; v < 3; ++v) grow(b, t[3 * v], t[3 * v + 1], t[3 * v + 2]);
@@ -185,10 +195,31 @@ __global__ void __launch_bounds__(256) noalloc_setup_kernel(const float *tri, co
         nc[k] = make_float4(cbx[0][2], cbx[0][5], cbx[1][2], cbx[1][5]);
         nd[k] = make_int4(ref[0], ref[1], 0, 0);
     }
+    __syncthreads();
+    if (tid == 0 && reinterpret_cast<unsigned long long *>(s + OFF_CNT)[LP_C_BAD_INPUT] != 0)
+        *reinterpret_cast<unsigned long long *>(s + OFF_WORK) = kRejectAll;
 }
 
 std::mutex g_mu;
 void *g_scratch_addr[256] = {};
+
+// The device address of the scratch array on the current device.  Outside stream
+// capture it is looked up again at every call (cheap), so a module reloaded after
+// cudaDeviceReset is followed; inside a capture the address cached by an earlier call
+// on this device is used, because the lookup may not be captured.
+int scratch_address(int dev, cudaStream_t s, void **out)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (cs == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return LP_ERR_CUDA;
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return LP_OK;
+}
 
 int reject(int code, const char *msg)
 {
@@ -220,33 +251,32 @@ extern "C" int lp_run_noalloc(const lp_noalloc_args *a, void *stream)
         if (!(a->det_grid[i] > 0.0f)) return reject(LP_ERR_INVALID, "lp_run_noalloc: detection grid step not positive");
     for (int i = 0; i < 4 * a->n_media; ++i)
         if (!std::isfinite(a->nmuasg[i])) return reject(LP_ERR_INVALID, "lp_run_noalloc: non-finite optical property");
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 256) return reject(LP_ERR_CUDA, "lp_run_noalloc: no current CUDA device");
-    void *base = nullptr;
-    {
-        // set-up once per device, with that device current: the device address of the
-        // scratch array (its name is only a host-side stand-in in host code)
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_addr[dev]) {
-            e = cudaGetSymbolAddress(&g_scratch_addr[dev], g_noalloc_scratch);
-            if (e != cudaSuccess) {
-                g_scratch_addr[dev] = nullptr;
-                return reject(LP_ERR_CUDA, "lp_run_noalloc: cudaGetSymbolAddress failed");
-            }
-        }
-        base = g_scratch_addr[dev];
-    }
-    if (a->n_photons == 0) return LP_OK;
-    unsigned char *sb = static_cast<unsigned char *>(base);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-
-    // tally-image extents (CalculatePropagation::InitLogVectors, CP.cpp:127-131)
+    for (int i = 0; i < 3; ++i)
+        if (!(std::isfinite(a->dimensions[i]) && a->dimensions[i] > 0.0f))
+            return reject(LP_ERR_INVALID, "lp_run_noalloc: model dimensions must be finite and positive");
+    // tally-image extents (CalculatePropagation::InitLogVectors, CP.cpp:127-131), bounded
+    // in double before the int casts: the kernel indexes the caller's sft, rtd and rz
+    // buffers with them, and their sizes cannot be checked here
+    const double kMaxExtent = double(1 << 20);
+    for (int i = 0; i < 3; ++i)
+        if (!((double)a->dimensions[i] / (double)a->det_grid[i] < kMaxExtent))
+            return reject(LP_ERR_RANGE, "lp_run_noalloc: image extent beyond 2^20 cells");
+    if (!(90.0 / (double)a->det_grid[5] < kMaxExtent)) return reject(LP_ERR_RANGE, "lp_run_noalloc: angle bins beyond 2^20");
     const int dimx = (int)(a->dimensions[0] / a->det_grid[0]), dimy = (int)(a->dimensions[1] / a->det_grid[1]);
     const int dimz = (int)(a->dimensions[2] / a->det_grid[2]), dimAlpha = (int)(90 / a->det_grid[5]);
     const int dimR = (int)std::ceil(std::sqrt(std::pow((double)(dimx / 2), 2) + std::pow((double)(dimy / 2), 2)));
     if (dimx < 0 || dimy < 0 || dimz < 0 || dimAlpha < 1 || dimR < 1)
         return reject(LP_ERR_RANGE, "lp_run_noalloc: image extents out of range");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 256) return reject(LP_ERR_CUDA, "lp_run_noalloc: no current CUDA device");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the scratch array's device address on this device (its name is only a host-side
+    // stand-in in host code)
+    void *base = nullptr;
+    if (scratch_address(dev, s, &base) != LP_OK) return reject(LP_ERR_CUDA, "lp_run_noalloc: cudaGetSymbolAddress failed");
+    if (a->n_photons == 0) return LP_OK;
+    unsigned char *sb = static_cast<unsigned char *>(base);
 
     if ((e = cudaMemsetAsync(sb, 0, HEADER, s)) != cudaSuccess) return reject(LP_ERR_CUDA, "lp_run_noalloc: memset");
     MediaParams mp;
@@ -300,7 +330,7 @@ extern "C" int lp_run_noalloc(const lp_noalloc_args *a, void *stream)
     P.key1 = (uint32_t)(a->seed >> 32);
     P.first = a->first;
     P.n = a->n_photons;
-    P.max_steps = 100000000;
+    P.max_steps = LP_NOALLOC_MAX_STEPS;
     P.hx = dimx / 2; P.hy = dimy / 2; P.sft_nx = 2 * (dimx / 2) + 1;
     P.dimR = dimR; P.dimAlpha = dimAlpha; P.rz_nr = 2 * dimR + 1; P.rz_nz = dimz + 1;
     for (int i = 0; i < 6; ++i) P.dg[i] = a->det_grid[i];
@@ -316,11 +346,16 @@ extern "C" int lp_run_noalloc(const lp_noalloc_args *a, void *stream)
     // voxel grid, radial bins, rings, exit records and the safety grid stay off
     const int smem = smem_bytes(P.nodes_smem, P.tris_smem);
     int per_sm = 0, sms = 148;
-    if ((e = transport_occupancy_exact(smem, &per_sm)) != cudaSuccess || per_sm < 1)
-        return reject(LP_ERR_CUDA, "lp_run_noalloc: occupancy query failed");
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if ((e = launch_transport_exact(P, sms * per_sm, smem, s)) != cudaSuccess)
-        return reject(LP_ERR_CUDA, "lp_run_noalloc: transport launch failed");
+    {
+        // the kernel's shared-memory attribute is process-wide: lp_run on another thread
+        // sets it too, so the setting and the launch are made under the same lock
+        std::lock_guard<std::mutex> lk(lp::launch_mutex());
+        if ((e = transport_occupancy_exact(smem, &per_sm)) != cudaSuccess || per_sm < 1)
+            return reject(LP_ERR_CUDA, "lp_run_noalloc: occupancy query failed");
+        if ((e = launch_transport_exact(P, sms * per_sm, smem, s)) != cudaSuccess)
+            return reject(LP_ERR_CUDA, "lp_run_noalloc: transport launch failed");
+    }
     if (a->counters) {
         e = cudaMemcpyAsync(a->counters, sb + OFF_CNT, LP_NCOUNTERS * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return reject(LP_ERR_CUDA, "lp_run_noalloc: counter copy failed");

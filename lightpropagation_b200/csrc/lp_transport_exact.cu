@@ -67,6 +67,21 @@ __global__ void __launch_bounds__(256) fma_peak_kernel(float *out, int iters, fl
     if (s == 1234.5f) out[0] = s;  // keeps the chains alive; practically never taken
 }
 
+// 64-bit atomic adds whose results are not used (reductions at the L2), each lane of a
+// warp to its own pseudo-random slot of an L2-resident buffer: the access pattern of the
+// transport kernel's absorption deposits.
+__global__ void __launch_bounds__(256) red_peak_kernel(unsigned long long *buf, uint32_t mask, int iters)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t h = g * 0x9E3779B1u + 0x7F4A7C15u;
+    for (int i = 0; i < iters; ++i) {
+        h ^= h >> 15;
+        h *= 0x2C1B3C6Du;
+        h ^= h >> 12;
+        atomicAdd(buf + (h & mask), 1ull);
+    }
+}
+
 int smem_bytes(int nodes_smem, int tris_smem) { return smem_layout(nodes_smem, tris_smem).bytes; }
 
 int block_size() { return kBlock; }
@@ -110,6 +125,35 @@ double fma_peak_tflops(int num_sms)
         cudaEventElapsedTime(&ms, e0, e1);
         const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
         if (ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    return best;
+}
+
+// Throughput of 64-bit atomic reductions to an L2-resident buffer (16 MB), in atomics/s.
+double red_peak_per_s(int num_sms)
+{
+    const uint32_t slots = 1u << 21;   // 16 MB of uint64
+    unsigned long long *d = nullptr;
+    if (cudaMalloc(&d, (size_t)slots * 8) != cudaSuccess) return 0.0;
+    cudaMemset(d, 0, (size_t)slots * 8);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = num_sms * 8, threads = 256, iters = 512;
+    red_peak_kernel<<<blocks, threads>>>(d, slots - 1, 16);   // warm-up
+    double best = 0.0;
+    for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(e0);
+        red_peak_kernel<<<blocks, threads>>>(d, slots - 1, iters);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double n = (double)iters * blocks * threads;
+        if (ms > 0) best = std::max(best, n / (ms * 1e-3));
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -53,6 +53,7 @@ struct Photon {
     int64_t pid;
     float seg_len;           // differentiation: path length and interactions in the
     uint32_t seg_k;          // current region since the photon entered it
+    float safe;              // lower bound of the distance from the position to any triangle
 };
 
 // Per-photon, per-region path lengths and interaction counts of a differentiated run
@@ -179,6 +180,17 @@ __device__ __forceinline__ float fresnel(float n1, float n2, float cosIn)
     return r;
 }
 
+// Sum of x over the lanes of grp (a __match_any_sync group, every lane of it calling),
+// exact for x < 2^59: the three slices x[0:16], x[16:32], x[32:64] are reduced by
+// redux.sync, and each slice's sum over at most 32 lanes fits in 32 bits.
+__device__ __forceinline__ unsigned long long group_sum_u64(unsigned grp, unsigned long long x)
+{
+    const unsigned a = __reduce_add_sync(grp, (unsigned)(x & 0xffffull));
+    const unsigned b = __reduce_add_sync(grp, (unsigned)((x >> 16) & 0xffffull));
+    const unsigned c = __reduce_add_sync(grp, (unsigned)(x >> 32));
+    return (unsigned long long)a + ((unsigned long long)b << 16) + ((unsigned long long)c << 32);
+}
+
 __device__ __forceinline__ void add_fix(unsigned long long *a, float w)
 {
     const unsigned long long f = fix32(w);
@@ -301,6 +313,7 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
     ph.pid = pid;
     ph.seg_len = 0.0f;
     ph.seg_k = 0;
+    ph.safe = 0.0f;
 }
 
 // One iteration of the reference's do-while loop.  Returns false when the photon ends.
@@ -309,10 +322,18 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
                                             unsigned long long *s_region, unsigned long long *s_cnt,
                                             Photon &ph, Counters &cnt, GradAcc *ga)
 {
-    // the cell word is read first so that its load overlaps the Philox rounds
-    const uint32_t word = cell_at(P, ph.px, ph.py, ph.pz);
+    // With no distance bound left (after a boundary, or once the steps have used it up)
+    // the step surely needs the cell word: its load is issued before the Philox rounds so
+    // that they hide its latency.  Otherwise it is read only if the step exceeds the bound.
+    const bool fresh = !(ph.safe > 0.0f);
+    uint32_t word = fresh ? cell_at(P, ph.px, ph.py, ph.pz) : 0u;
     EventRng rng;
     rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
+    [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
+    if (!LP_IN_RANGE(dbg, ph.curr, P.n_media)) {
+        ph.w = 0.0f;
+        return false;
+    }
     const Medium m = s_media[ph.curr];
     float step = 0.0f;
     if (!m.ambient) {
@@ -326,26 +347,51 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     }
     float thit;
     int tri;
+    // safe_here: lower bound of the distance from p to every triangle.  A step shorter
+    // than it cannot reach one, so its bounded query would return "no hit" and is skipped;
+    // after the step the bound shrinks by the step (plus the rounding of the move).
+    float safe_here = ph.safe;
     const V3 p = v3(ph.px, ph.py, ph.pz), v = v3(ph.vx, ph.vy, ph.vz);
     if (m.ambient) {
         tri = query_nearest<STACK>(M, p, v, ph.refTri, kNoHit, thit);
         cnt.query++;
         cnt.bvh++;
-    } else if (step < safe_distance(P, word)) {
-        // no triangle within the step: the bounded query would return "no hit"
+    } else if (step < safe_here) {
         tri = -1;
         thit = kNoHit;
         cnt.skip++;
     } else {
-        bool used_bvh;
-        tri = cell_query<STACK>(P, M, p, v, ph.refTri, step, thit, used_bvh);
-        cnt.query++;
-        cnt.bvh += used_bvh ? 1u : 0u;
+        if (!fresh) word = cell_at(P, ph.px, ph.py, ph.pz);
+        bool done = false;
+        if (word & kCellEmpty) {
+            // a cell no triangle touches: its word holds a bound for all its points
+            safe_here = safe_distance(P, word);
+            if (step < safe_here) {
+                tri = -1;
+                thit = kNoHit;
+                cnt.skip++;
+                done = true;
+            }
+        } else if (P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
+            // the cell's own list: a bound from the planes of its triangles, and the
+            // query itself when the step stays inside the widened cell
+            done = list_query(P, M, p, v, ph.refTri, step, word, thit, tri, safe_here);
+            if (done) cnt.query++;
+        } else {
+            safe_here = 0.0f;
+        }
+        if (!done) {
+            bool used_bvh;
+            tri = cell_query<STACK>(P, M, p, v, ph.refTri, step, thit, used_bvh);
+            cnt.query++;
+            cnt.bvh += used_bvh ? 1u : 0u;
+        }
     }
     if (m.ambient) step = thit;
     const bool boundary = (tri >= 0) ? (thit <= step) : (kNoHit <= step);
     if (boundary) {
         cnt.boundary++;
+        ph.safe = 0.0f;
         ph.px = ph.px + thit * ph.vx;
         ph.py = ph.py + thit * ph.vy;
         ph.pz = ph.pz + thit * ph.vz;
@@ -355,12 +401,13 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             // the reference would read mediumIDs[-1] here; the photon leaves the model
             atomicAdd(s_cnt + 4, 1ull);
             ph.w = 0.0f;
-        } else {
+        } else if (LP_IN_RANGE(dbg, tri, P.n_tri)) {
             const float4 at = __ldg(P.tri_attr + tri);
             const int ids = __float_as_int(at.w);
             const int inner = ids & 0xffff, outer = ids >> 16;
             V3 nv = v3(at.x, at.y, at.z);
-            const int nxt_id = (ph.curr == outer) ? inner : outer;
+            int nxt_id = (ph.curr == outer) ? inner : outer;
+            if (!LP_IN_RANGE(dbg, nxt_id, P.n_media)) nxt_id = ph.curr;
             const Medium nx = s_media[nxt_id];
             if (P.compat & 0x2u) {
                 if (fabsf(sqrtf(ph.px * ph.px + ph.py * ph.py)) < 0.01f) {
@@ -445,6 +492,8 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             } else if (Grad) {
                 ph.seg_len += thit;
             }
+        } else {
+            ph.w = 0.0f;   // debug build: a triangle index out of range ends the photon
         }
     } else {
         cnt.scatter++;
@@ -452,6 +501,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.py = ph.py + step * ph.vy;
         ph.pz = ph.pz + step * ph.vz;
         ph.refTri = -1;
+        ph.safe = fmaxf(safe_here - step - P.step_eps, 0.0f);
         if (Grad) {
             ph.seg_len += step;
             ph.seg_k++;
@@ -479,13 +529,9 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             row = (int)floorf(cz * P.inv_dz);
             col = (int)floorf(rad + (float)P.dimR);
         }
-        if (row >= 0 && row < P.rz_nz && col >= 0 && col < P.rz_nr) {
-            unsigned long long *c = P.rz + 2 * ((int64_t)row * P.rz_nr + col);
-            if (fdw) atomicAdd(c, fdw);
-            if (m.mua > 0.0f) add_fix(c + 1, Exact ? dw / m.mua : dw * m.inv_mua);
-        } else {
-            cnt.rz_drop++;
-        }
+        const bool rz_in = row >= 0 && row < P.rz_nz && col >= 0 && col < P.rz_nr;
+        const unsigned long long fdm = (m.mua > 0.0f) ? fix32(Exact ? dw / m.mua : dw * m.inv_mua) : 0ull;
+        int vox_key = -1;
         if (P.vox_nx > 0) {
             int ix, iy, iz;
             if (Exact) {
@@ -497,11 +543,40 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
                 iy = (int)floorf(cy * P.inv_vdy + 0.5f * (float)P.vox_ny);
                 iz = (int)floorf(cz * P.inv_vdz);
             }
-            if (ix >= 0 && ix < P.vox_nx && iy >= 0 && iy < P.vox_ny && iz >= 0 && iz < P.vox_nz) {
-                if (fdw) atomicAdd(P.vox + ((int64_t)iz * P.vox_ny + iy) * P.vox_nx + ix, fdw);
-            } else {
+            if (ix >= 0 && ix < P.vox_nx && iy >= 0 && iy < P.vox_ny && iz >= 0 && iz < P.vox_nz)
+                vox_key = (iz * P.vox_ny + iy) * P.vox_nx + ix;
+            else
                 cnt.vox_drop++;
+        }
+        if (!rz_in) cnt.rz_drop++;
+        const int rz_key = rz_in ? row * P.rz_nr + col : -1;
+        if (P.agg_tallies) {
+            // warp-aggregated deposits: the lanes of this branch that hit the same cell
+            // are matched, their fixed-point values summed exactly, and one leader per
+            // cell issues the atomic add (integer sums: same tallies as the plain form)
+            const unsigned lane = threadIdx.x & 31u;
+            const unsigned act = __activemask();
+            const unsigned g_rz = __match_any_sync(act, rz_key);
+            if (rz_key >= 0) {
+                const unsigned long long a = group_sum_u64(g_rz, fdw), b = group_sum_u64(g_rz, fdm);
+                if (lane == (unsigned)(__ffs(g_rz) - 1)) {
+                    unsigned long long *c = P.rz + 2 * (int64_t)rz_key;
+                    if (a) atomicAdd(c, a);
+                    if (b) atomicAdd(c + 1, b);
+                }
             }
+            const unsigned g_vox = __match_any_sync(act, vox_key);
+            if (vox_key >= 0) {
+                const unsigned long long a = group_sum_u64(g_vox, fdw);
+                if (a && lane == (unsigned)(__ffs(g_vox) - 1)) atomicAdd(P.vox + vox_key, a);
+            }
+        } else {
+            if (rz_key >= 0) {
+                unsigned long long *c = P.rz + 2 * (int64_t)rz_key;
+                if (fdw) atomicAdd(c, fdw);
+                if (fdm) atomicAdd(c + 1, fdm);
+            }
+            if (vox_key >= 0 && fdw) atomicAdd(P.vox + vox_key, fdw);
         }
         ph.region_acc += fdw;
     }
@@ -567,6 +642,9 @@ __device__ __forceinline__ MeshView stage_mesh(const KParams &P, unsigned char *
     M.s_ta = ta; M.s_tb = tb; M.s_tc = tc;
     M.nodes_smem = P.nodes_smem;
     M.tris_smem = P.tris_smem;
+    M.n_nodes = P.n_nodes;
+    M.n_tri = P.n_tri;
+    M.dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
     return M;
 }
 

@@ -184,6 +184,16 @@ class Simulation:
         results are unchanged either way)."""
         self._ck(self._L.lp_set_cell_lists(self._h, 1 if enable else 0))
 
+    def set_cell_margin(self, cells: float):
+        """Margin of the cell lists in cells (default 0.5): each list holds the triangles
+        touching its cell widened by this much (results are unchanged)."""
+        self._ck(self._L.lp_set_cell_margin(self._h, float(cells)))
+
+    def set_tally_aggregation(self, enable: bool):
+        """Sum same-cell absorption deposits across the warp before the atomic adds
+        (tallies are identical either way)."""
+        self._ck(self._L.lp_set_tally_aggregation(self._h, 1 if enable else 0))
+
     def set_smem_budget(self, nbytes: int):
         """Shared memory per block for staged BVH nodes and triangles (the rest is L1)."""
         self._ck(self._L.lp_set_smem_budget(self._h, int(nbytes)))
@@ -225,6 +235,40 @@ class Simulation:
         self._ck(self._L.lp_get_tallies(self._h, C.byref(T)))
         return tallies_dict(T, g)
 
+    # -- checkpoint / resume (lp_set_tallies, lp_get/set_gradient_sums)
+    def checkpoint(self) -> dict:
+        """The integer tallies, the counters and the differentiation sums.  With the seed
+        and the id of the next photon that is all a resumed run needs: photon streams
+        depend on the seed and the photon id alone."""
+        g = self.geometry()
+        T = N.Tallies()
+        self._ck(self._L.lp_get_tallies(self._h, C.byref(T)))
+        t = tallies_dict(T, g)
+        ck = {k: t[k].copy() for k in ("sft", "rtd", "rz", "vox", "rbins", "region", "det")}
+        ck["counters"] = np.array([T.counters[i] for i in range(N.NCOUNTERS)], np.uint64)
+        n = int(t["det"].shape[0]) * self._n_media * 5
+        ck["grad"] = np.zeros(n, np.float64)
+        if n:
+            self._ck(self._L.lp_get_gradient_sums(self._h, ck["grad"].ctypes.data_as(C.POINTER(C.c_double)), n))
+        return ck
+
+    def restore(self, ck: dict):
+        """Replace this context's tallies, counters and differentiation sums by a checkpoint
+        taken with the same tally layout."""
+        arrs = {k: np.ascontiguousarray(ck[k], np.uint64) for k in ("sft", "rtd", "rz", "vox", "rbins", "region",
+                                                                    "det")}
+        T = N.Tallies()
+        for k, a in arrs.items():
+            setattr(T, k, a.ctypes.data_as(C.POINTER(C.c_uint64)))
+        for i in range(N.NCOUNTERS):
+            T.counters[i] = int(ck["counters"][i])
+        T.n_vox, T.n_rbins = arrs["vox"].size, arrs["rbins"].shape[0]
+        T.n_region, T.n_det = arrs["region"].size, arrs["det"].shape[0]
+        self._ck(self._L.lp_set_tallies(self._h, C.byref(T)))
+        g = np.ascontiguousarray(ck.get("grad", np.zeros(0)), np.float64)
+        if g.size:
+            self._ck(self._L.lp_set_gradient_sums(self._h, g.ctypes.data_as(C.POINTER(C.c_double)), g.size))
+
     def stats(self) -> dict:
         st = N.Stats()
         self._ck(self._L.lp_get_stats(self._h, C.byref(st)))
@@ -256,6 +300,13 @@ def fp32_peak_tflops(device: int = 0) -> float:
     """Measured FP32 FMA throughput of the device (TFLOP/s)."""
     t = C.c_double()
     N.check(N.lib().lp_fp32_peak(device, C.byref(t)))
+    return float(t.value)
+
+
+def l2_atomic_peak(device: int = 0) -> float:
+    """Measured throughput of 64-bit atomic adds to an L2-resident buffer (atomics/s)."""
+    t = C.c_double()
+    N.check(N.lib().lp_l2_atomic_peak(device, C.byref(t)))
     return float(t.value)
 
 
@@ -316,6 +367,7 @@ class CalculatePropagation:
         self.triN = None
         self.vStart, self.vStartOcc, self.pStart = None, None, None
         self.seed = 0x4C50
+        self.exact = False                 # reference-order arithmetic (lp_set_arithmetic)
         self.compat = N.COMPAT_ALL
         self.extra = None
         self._sim: Optional[Simulation] = None
@@ -336,6 +388,7 @@ class CalculatePropagation:
     def SetFetalTissueID(self, i): self.fetalTissueID = int(i)
     def SetDimensions(self, dims): self.dimensions = [float(x) for x in dims]
     def SetSeed(self, seed): self.seed = int(seed)
+    def SetArithmetic(self, exact): self.exact = bool(exact)
     def SetCompat(self, compat): self.compat = int(compat)
 
     def SetDetectionGridDimensions(self, *grid):
@@ -396,6 +449,7 @@ class CalculatePropagation:
         s.set_source(self.pStart, self.vStart, self.eP0XYZ, self.vStartOcc)
         s.set_tally_grid(self.dimensions, self.DetGridDims, self.fetalTissueID)
         s.set_params(self.chance, self.w_threshold, self.pixelPerUnitFactor, self.seed, self.compat)
+        s.set_arithmetic(self.exact)
         if self.extra:
             s.set_extra_tallies(**self.extra)
         s.zero()

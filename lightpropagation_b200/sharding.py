@@ -8,7 +8,9 @@ is a uint64 fixed-point sum (2^32 per unit weight), and integer addition is asso
 and commutative, so the tallies summed over ranks equal the single-GPU tallies bit for
 bit.  That sum is the path's only collective: one all-reduce of one flat int64 buffer
 per launch (NCCL over NVLink on GPUs, gloo on CPU for tests).  uint64 values travel as
-int64; two's-complement addition wraps exactly like uint64 addition.
+int64; two's-complement addition wraps exactly like uint64 addition.  A differentiated
+run adds the FP64 perturbation sums, reduced in a second, float64 all-reduce: those
+agree with one GPU's to rounding, not bit for bit.
 
 This replaces nothing in the reference, which runs on one OpenCL device
 (CalculatePropagation.cpp:1389-1759); the photon loop it splits into 6400-photon
@@ -36,51 +38,65 @@ def photon_range(n: int, rank: int, world: int, first: int = 0) -> Tuple[int, in
 
 
 def allreduce_flat(tensors: List["object"], group=None) -> None:
-    """Sum int64 tensors over the process group in place with ONE all-reduce: pack them
-    into a flat buffer on their device, reduce it, unpack."""
+    """Sum tensors over the process group in place with one all-reduce per dtype (int64
+    tallies; float64 differentiation sums, if any): pack each dtype's tensors into a
+    flat buffer on their device, reduce it, unpack."""
     import torch
     import torch.distributed as dist
     if not tensors:
         return
     for t in tensors:
-        if t.dtype != torch.int64:
-            raise TypeError("tallies are reduced as int64")
-    flat = torch.cat([t.reshape(-1) for t in tensors])
-    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
-    off = 0
-    for t in tensors:
-        k = t.numel()
-        t.view(-1).copy_(flat[off:off + k])
-        off += k
+        if t.dtype not in (torch.int64, torch.float64):
+            raise TypeError("tallies are reduced as int64, differentiation sums as float64")
+    for dt in (torch.int64, torch.float64):
+        part = [t for t in tensors if t.dtype == dt]
+        if not part:
+            continue
+        flat = torch.cat([t.reshape(-1) for t in part])
+        dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+        off = 0
+        for t in part:
+            k = t.numel()
+            t.view(-1).copy_(flat[off:off + k])
+            off += k
 
 
 def reduce_host_tallies(tallies: Dict[str, object], group=None) -> Dict[str, object]:
-    """Sum host tallies (numpy uint64 arrays and the ``counters`` dict) over the group.
-    Returns a new dict with the same keys and shapes; the inputs are not modified."""
+    """Sum host tallies (numpy uint64 arrays, the ``counters`` dict and, if present, the
+    float64 ``grad`` differentiation sums) over the group.  Returns a new dict with the
+    same keys and shapes; the inputs are not modified."""
     import torch
     keys = [k for k in TALLY_KEYS if k in tallies]
     arrays = [np.ascontiguousarray(tallies[k], np.uint64) for k in keys]
     names = sorted(tallies["counters"]) if "counters" in tallies else []
     cnt = np.array([tallies["counters"][k] for k in names], np.uint64)
     ts = [torch.from_numpy(a.view(np.int64).copy()) for a in arrays + [cnt]]
+    grad = None
+    if tallies.get("grad") is not None:
+        grad = torch.from_numpy(np.array(tallies["grad"], np.float64, copy=True))
+        ts.append(grad)
     allreduce_flat(ts, group)
     out = {k: t.numpy().view(np.uint64).reshape(a.shape) for k, a, t in zip(keys, arrays, ts)}
     if names:
-        out["counters"] = {k: int(v) for k, v in zip(names, ts[-1].numpy().view(np.uint64))}
+        out["counters"] = {k: int(v) for k, v in zip(names, ts[len(arrays)].numpy().view(np.uint64))}
+    if grad is not None:
+        out["grad"] = grad.numpy()
     return out
 
 
 class _DeviceArray:
     """A raw device pointer seen by torch through __cuda_array_interface__."""
 
-    def __init__(self, ptr: int, count: int):
-        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<i8", "data": (int(ptr), False),
+    def __init__(self, ptr: int, count: int, typestr: str = "<i8"):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3}
 
 
 def device_tally_tensors(sim, device: int) -> List["object"]:
     """The context's device tally buffers (and counters) as int64 torch tensors that alias
-    them; valid until the tally layout changes (lp_set_tally_grid / lp_set_extra_tallies)."""
+    them, plus the differentiation sums as one float64 tensor while differentiation is on;
+    valid until the tally layout changes (lp_set_tally_grid / lp_set_extra_tallies) or
+    differentiation is switched."""
     import torch
     d = sim.device_tallies()
     out = []
@@ -88,6 +104,8 @@ def device_tally_tensors(sim, device: int) -> List["object"]:
         cnt = getattr(d, "n_" + name)
         if cnt > 0:
             out.append(torch.as_tensor(_DeviceArray(getattr(d, name), cnt), device=f"cuda:{device}"))
+    if d.n_grad > 0:
+        out.append(torch.as_tensor(_DeviceArray(d.grad, d.n_grad, "<f8"), device=f"cuda:{device}"))
     return out
 
 

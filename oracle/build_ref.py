@@ -2,9 +2,10 @@
 """Build recipe for oracle/_ref/libclref.so: the reference's own kernel on the CPU.
 
 TEST INFRASTRUCTURE ONLY.  Reads the reference sources where they lie (under the
-reference checkout given by --reference, default /root/reference) and writes every
-output into oracle/_ref/, which is git-ignored.  Nothing is copied into the
-repository's history.
+reference checkout given by --reference, else the LP_REFERENCE_DIR environment
+variable, else /root/reference) and writes every output into oracle/_ref/, which is
+git-ignored.  Nothing is copied into the repository's history.  reference_dir() is
+the one place the default location is named; the tests and the build step ask it.
 
 Steps
   1. src/Simulation/MCLightPropagation.cl is read and the OpenCL vector literals
@@ -30,19 +31,30 @@ OUT = os.path.join(HERE, "_ref")
 VEC_LITERAL = re.compile(r"\((u?(?:char|short|int|long|float|double)(?:2|3|4|8|16))\)\s*\(")
 
 
+def reference_dir() -> str:
+    """The reference checkout: $LP_REFERENCE_DIR, else /root/reference."""
+    return os.environ.get("LP_REFERENCE_DIR") or "/root/reference"
+
+
+def reference_present(root: str = "") -> bool:
+    return os.path.isfile(os.path.join(root or reference_dir(), "src", "Simulation", "MCLightPropagation.cl"))
+
+
 def rewrite(src: str) -> str:
     return VEC_LITERAL.sub(lambda m: m.group(1) + "(", src)
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=reference_dir())
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     cl = os.path.join(a.reference, "src", "Simulation", "MCLightPropagation.cl")
     psnr_dir = os.path.join(a.reference, "src", "PSNR")
     if not os.path.isfile(cl):
-        print(f"build_ref: reference kernel not found at {cl}; skipping", file=sys.stderr)
+        print(f"build_ref: reference kernel not found at {cl} (set LP_REFERENCE_DIR); the live pin "
+              f"oracle/_ref is not built, the committed fixtures in tests/golden/ still pin the oracle",
+              file=sys.stderr)
         return 0
     os.makedirs(OUT, exist_ok=True)
     so = os.path.join(OUT, "libclref.so")

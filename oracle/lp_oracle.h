@@ -168,6 +168,27 @@ int lpo_run(const lpo_problem *P, int64_t first, int64_t n, int nthreads,
 /* Fixed-point encoding of a non-negative weight. */
 uint64_t lpo_fix(float w);
 
+/* ---- FP64 error oracle (lp_oracle64.c) ------------------------------------------
+ * The same physics, tallies and Philox draw layout as lpo_run with every quantity in
+ * double precision; the nearest-triangle search runs over a bounding-volume tree and
+ * returns the brute-force scan's answer (nearest t, then lowest index).  Only the
+ * LPO_RNG_PHILOX mode exists.  exit_rec receives the records rounded to float; rz_ref
+ * is not produced.  Tally arrays must be zeroed by the caller; results are added. */
+typedef struct lpo64_mesh lpo64_mesh;
+lpo64_mesh *lpo64_mesh_build(const float *tri, int32_t n_tri);
+void lpo64_mesh_free(lpo64_mesh *m);
+/* Nearest triangle along (p, v) with 0 < t <= bound and t < 10000, ref_tri excluded:
+ * through the tree, and by the brute-force scan of .cl:1037-1093 in double. */
+int32_t lpo64_mesh_query(const lpo64_mesh *m, int32_t ref_tri, const double p[3], const double v[3],
+                         double bound, double *t_out);
+int32_t lpo64_find_triangle(const float *tri, int32_t n_tri, int32_t ref_tri, const double p[3],
+                            const double v[3], double bound, double *t_out);
+double lpo64_fresnel(double n1, double n2, double cos_in);
+/* Trace photons [first, first+n) in FP64; mesh may be NULL (built and freed here).
+ * Returns 0, or 1 if the problem is not in the Philox mode or has too many regions. */
+int lpo64_run(const lpo_problem *P, const lpo64_mesh *mesh, int64_t first, int64_t n, int nthreads,
+              lpo_tallies *T);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,19 @@ def lib():
         L.lpo_find_triangle.restype = C.c_int32
         L.lpo_fix.argtypes = [C.c_float]
         L.lpo_fix.restype = C.c_uint64
+        _dp = C.POINTER(C.c_double)
+        L.lpo64_mesh_build.argtypes = [_fp, C.c_int32]
+        L.lpo64_mesh_build.restype = C.c_void_p
+        L.lpo64_mesh_free.argtypes = [C.c_void_p]
+        L.lpo64_mesh_query.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, C.c_double, _dp]
+        L.lpo64_mesh_query.restype = C.c_int32
+        L.lpo64_find_triangle.argtypes = [_fp, C.c_int32, C.c_int32, _dp, _dp, C.c_double, _dp]
+        L.lpo64_find_triangle.restype = C.c_int32
+        L.lpo64_fresnel.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.lpo64_fresnel.restype = C.c_double
+        L.lpo64_run.argtypes = [C.POINTER(Problem), C.c_void_p, C.c_int64, C.c_int64, C.c_int,
+                                C.POINTER(Tallies)]
+        L.lpo64_run.restype = C.c_int
         _lib = L
     return _lib
 
@@ -272,6 +285,77 @@ def run(case: Case, n: int, first: int = 0, rng_mode=RNG_PHILOX, seed=0x4C50,
     counters = {k: int(T.counters[i]) for i, k in enumerate(COUNTER_NAMES)}
     return Result(sft, rtd, rz, vox[:nv] if nv else vox[:0], rbins[:case.n_rbins], region,
                   det[:ndet], counters, rec, rzref, st, ix, grad[:ndet])
+
+
+class Mesh64:
+    """The FP64 oracle's bounding-volume tree over a mesh (float32 [T, 9] triangles)."""
+
+    def __init__(self, tri):
+        self.tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        self.handle = lib().lpo64_mesh_build(fptr(self.tri), self.tri.shape[0])
+
+    def query(self, p, v, ref_tri=-1, bound=10000.0):
+        """(index or -1, distance) of the nearest triangle with 0 < t <= bound."""
+        dp = C.POINTER(C.c_double)
+        pp = np.ascontiguousarray(p, np.float64)
+        vv = np.ascontiguousarray(v, np.float64)
+        t = np.zeros(1, np.float64)
+        j = lib().lpo64_mesh_query(self.handle, int(ref_tri), pp.ctypes.data_as(dp), vv.ctypes.data_as(dp),
+                                   float(bound), t.ctypes.data_as(dp))
+        return int(j), float(t[0])
+
+    def brute(self, p, v, ref_tri=-1, bound=10000.0):
+        """The same query by the brute-force scan."""
+        dp = C.POINTER(C.c_double)
+        pp = np.ascontiguousarray(p, np.float64)
+        vv = np.ascontiguousarray(v, np.float64)
+        t = np.zeros(1, np.float64)
+        j = lib().lpo64_find_triangle(fptr(self.tri), self.tri.shape[0], int(ref_tri), pp.ctypes.data_as(dp),
+                                      vv.ctypes.data_as(dp), float(bound), t.ctypes.data_as(dp))
+        return int(j), float(t[0])
+
+    def close(self):
+        if self.handle:
+            lib().lpo64_mesh_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def run64(case: Case, n: int, first: int = 0, seed=0x4C50, compat=COMPAT_ALL, nthreads=0, stream=0,
+          exit_records=False, max_steps=0, mesh: Optional[Mesh64] = None) -> Result:
+    """Trace photons [first, first+n) with the FP64 oracle (Philox draws, same tallies)."""
+    g = geometry(case)
+    P = case.problem(RNG_PHILOX, seed, compat, stream, max_steps)
+    sft = np.zeros((g.sft_ny, g.sft_nx, 3), np.uint64)
+    rtd = np.zeros((g.dimAlpha, g.dimR, 3), np.uint64)
+    rz = np.zeros((g.rz_nz, g.rz_nr, 2), np.uint64)
+    nv = int(np.prod(case.vox_n)) if case.vox_n[0] > 0 else 0
+    vox = np.zeros((max(nv, 1),), np.uint64)
+    rbins = np.zeros((max(case.n_rbins, 1), 2), np.uint64)
+    region = np.zeros((case.nmuasg.shape[0],), np.uint64)
+    ndet = 0 if case.det_r is None else case.det_r.shape[0]
+    det = np.zeros((max(ndet, 1), 2), np.uint64)
+    T = Tallies()
+    T.sft, T.rtd, T.rz, T.vox = uptr(sft), uptr(rtd), uptr(rz), uptr(vox)
+    T.rbins, T.region, T.det = uptr(rbins), uptr(region), uptr(det)
+    grad = np.zeros((max(ndet, 1), case.nmuasg.shape[0], 5), np.float64)
+    if ndet:
+        T.grad = grad.ctypes.data_as(C.POINTER(C.c_double))
+    rec = None
+    if exit_records:
+        rec = np.zeros((n, 8), np.float32)
+        T.exit_rec = fptr(rec)
+    rc = lib().lpo64_run(C.byref(P), mesh.handle if mesh is not None else None, first, n, nthreads, C.byref(T))
+    if rc != 0:
+        raise ValueError("lpo64_run: the FP64 oracle needs the Philox mode and at most 64 regions")
+    counters = {k: int(T.counters[i]) for i, k in enumerate(COUNTER_NAMES)}
+    return Result(sft, rtd, rz, vox[:nv] if nv else vox[:0], rbins[:case.n_rbins], region,
+                  det[:ndet], counters, rec, None, None, None, grad[:ndet])
 
 
 def ran3_init(seed: int):

@@ -14,7 +14,7 @@ ImportExport::GenMediumIDsFromObjModel (src/IO/ImportExport.cpp:952-1053): regio
 ids from `o <name>` / `g <id>` / `g <id>_<surf>` lines, one triangle per `f` line,
 per-face normal (B - A) x (C - A).  Only this script reads the reference checkout.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference DIR] [case ...]   (DIR: $LP_REFERENCE_DIR)
 """
 import argparse
 import os
@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import pyoracle as po  # noqa: E402
+from build_ref import reference_dir  # noqa: E402
 from lightpropagation_b200 import meshes  # noqa: E402
 
 CASES = [
@@ -38,7 +39,19 @@ CASES = [
     ("model2", "model2", "model.obj", "config.xml", 1500, 77),
     ("model3", "model3", "model.obj", "config.xml", 1500, 4242),
     ("model4_planar", "model4", "modelPlanar.obj", "configPlanar.xml", 600, 31),
+    # the curved 5-region model (25,600 triangles); its mesh is stored as shared vertices
+    # and faces, which arrays() expands
+    ("model4_curved", "model4", "model.obj", "config.xml", 400, 8),
 ]
+
+
+def arrays(z):
+    """(tri [T, 9], nrm [T, 3], med [T, 2]) of a fixture: stored directly, or as shared
+    vertices + faces with the per-face normals (B - A) x (C - A) recomputed."""
+    if "tri" in z:
+        return z["tri"], z["nrm"], z["med"]
+    tri = z["verts"][z["faces"]].reshape(-1, 9).astype(np.float32)
+    return tri, meshes.face_normals(tri), z["med"]
 
 
 def read_config(path):
@@ -69,7 +82,7 @@ def read_config(path):
                 chance=chance, wth=wth, det=det, fetal=fetal)
 
 
-def read_obj(path, names):
+def read_obj(path, names, indexed=False):
     verts, faces, med = [], [], []
     inner = outer = 0
     with open(path) as fh:
@@ -99,13 +112,15 @@ def read_obj(path, names):
                 outer = int(m.group(1))
     v = np.array(verts, np.float32)
     tri = np.stack([np.concatenate([v[a], v[b], v[c]]) for a, b, c in faces]).astype(np.float32)
+    if indexed:
+        return tri, meshes.face_normals(tri), np.array(med, np.int32), v, np.array(faces, np.int32)
     return tri, meshes.face_normals(tri), np.array(med, np.int32)
 
 
 def make_case(ref_root, name, mdir, obj, cfg, n, seed):
     c = read_config(os.path.join(ref_root, "models", mdir, cfg))
     names = [t[1] for t in c["tissues"]]
-    tri, nrm, med = read_obj(os.path.join(ref_root, "models", mdir, obj), names)
+    tri, nrm, med, verts, faces = read_obj(os.path.join(ref_root, "models", mdir, obj), names, indexed=True)
     nmuasg = np.array([[t[2], t[3], t[4], t[5]] for t in c["tissues"]], np.float32)
     ex, ey, ez = meshes.emitter_frame(c["head"])
     p0 = meshes.emitter_start(c["pos"], c["head"], c["dist"])
@@ -119,8 +134,11 @@ def make_case(ref_root, name, mdir, obj, cfg, n, seed):
     st0, ix0 = po.ref_ran3_state(seed)
     rec, rz, st, ix = po.ref_run(case, n, ran3_seed=seed, rz_pad=pad)
     cells = np.nonzero(np.any(rz != 0, axis=1))[0]
-    out = dict(tri=tri, nrm=nrm, med=med, nmuasg=nmuasg, p_start=p0, v_start=case.v_start, ep0xyz=ep,
+    mesh = dict(tri=tri, nrm=nrm, med=med) if tri.shape[0] < 1000 else dict(verts=verts, faces=faces, med=med)
+    out = dict(**mesh, nmuasg=nmuasg, p_start=p0, v_start=case.v_start, ep0xyz=ep,
                dimensions=case.dimensions, det_grid=case.det_grid,
+               emitter=np.array(c["pos"] + c["head"] + [c["dist"]], np.float32),
+               tissue_names=np.array(names),
                scalars=np.array([c["fetal"], c["chance"], c["wth"], c["ppu"], n, seed, pad], np.float64),
                ran3_state0=st0, ran3_inext0=ix0, exit_rec=rec,
                rz_cells=(cells - pad).astype(np.int64), rz_vals=rz[cells], ran3_state1=st, ran3_inext1=ix)
@@ -131,7 +149,8 @@ def make_case(ref_root, name, mdir, obj, cfg, n, seed):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=reference_dir())
+    ap.add_argument("cases", nargs="*", help="names of the cases to make (default: all)")
     a = ap.parse_args()
     if not po.ref_available():
         import subprocess
@@ -139,7 +158,8 @@ def main():
                                "--reference", a.reference])
     po.build()
     for case in CASES:
-        make_case(a.reference, *case)
+        if not a.cases or case[0] in a.cases:
+            make_case(a.reference, *case)
 
 
 if __name__ == "__main__":

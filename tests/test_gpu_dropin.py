@@ -1,0 +1,158 @@
+"""The drop-in boundary on the GPU with the reference's own models (marked gpu).
+
+The reference's main flow (src/main/main.cpp:174-332) is: read the config, the OBJ mesh
+and the emitter file; set them on CalculatePropagation (CalculatePropagation.hpp:212-388);
+Init(); Propagation(); then hand the Get*Image() results to Analysis and Logs.  Here that
+flow runs on the reference's shipped models (models/model1, model3, the planar and the
+curved 25,600-triangle model4; their kernel inputs are committed under tests/golden/ by
+make_golden.py), written back to reference-format files in a temporary directory:
+
+  * the C++ launcher (lp::CalculatePropagation in liblphost.so) through lpsim, which
+    writes the reference's log files from the GPU tallies;
+  * the Python launcher (lightpropagation_b200.CalculatePropagation) with the same
+    setters and seed, whose images, written by the same log writers, must give the
+    same files byte for byte;
+  * the images against the oracle with common random numbers: reference-order
+    arithmetic on the GPU, the same Philox stream in the oracle (the FP32 restatement
+    that is pinned to the reference kernel; the FP64 oracle for the curved model, where
+    the FP32 oracle's brute-force scan of 25,600 triangles is too slow).
+"""
+import ctypes as C
+import filecmp
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import pyoracle as po  # noqa: E402
+from make_golden import arrays  # noqa: E402
+from lightpropagation_b200 import CalculatePropagation, meshes, modelio  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+MODELS = ["model1", "model3", "model4_planar", "model4_curved"]
+PHOTONS = {"model1": 50000, "model3": 50000, "model4_planar": 20000, "model4_curved": 20000}
+SEED = 0xD0C
+
+
+def write_model(name, d, photons):
+    """The fixture's model as reference-format files (config XML, OBJ, emitter file)."""
+    z = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    tri, _, med = arrays(z)
+    names = [str(x) for x in z["tissue_names"]]
+    s = z["scalars"]
+    em = z["emitter"]
+    meshes.write_obj(os.path.join(d, "model.obj"), tri, med, names)
+    with open(os.path.join(d, "emitter.txt"), "w") as f:
+        f.write("0 1\n")
+    tissues = [(nm, *z["nmuasg"][i]) for i, nm in enumerate(names)]
+    meshes.write_config(os.path.join(d, "config.xml"), "model.obj", tissues, z["dimensions"], z["det_grid"],
+                        em[0:3], em[3:6], em[6], photons, int(s[0]), chance=np.float32(s[1]),
+                        w_threshold=np.float32(s[2]), ppu=np.float32(s[3]))
+    return z, os.path.join(d, "config.xml")
+
+
+def python_launcher(w, photons, seed, exact):
+    """main.cpp's setter sequence on the Python launcher."""
+    cp = CalculatePropagation(0)
+    nm = w.nmuasg
+    cp.SetTissueProperties(nm[:, 0], nm[:, 1], nm[:, 3], nm[:, 2])
+    cp.SetFetalTissueID(w.fetal_id)
+    cp.SetDimensions(w.dimensions)
+    cp.SetDetectionGridDimensions(w.det_grid)
+    cp.SetTriangles(w.tri)
+    cp.SetNormals(w.nrm)
+    cp.SetInnerAndOuterTissueIndices(w.med)
+    cp.SetPixelPerUnitFactor(w.factor)
+    cp.SetStartTrajectories(w.v_start, [1])
+    cp.SetStartPoint(w.p_start)
+    cp.SetPOI(w.ep0xyz[0:3])
+    cp.SetBasisVectors(w.ep0xyz[3:6], w.ep0xyz[6:9], w.ep0xyz[9:12])
+    cp.SetChanceForRoulette(w.chance)
+    cp.SetWeightThreshold(w.w_threshold)
+    cp.SetNumberOfPhotons(photons)
+    cp.SetSeed(seed)
+    cp.SetArithmetic(exact)
+    assert cp.Init() == 0
+    assert cp.Propagation() == 0
+    return cp
+
+
+def write_logs(cp, d, grid, photons):
+    """The log files lpsim writes, from the Python launcher's images (same writers)."""
+    L = modelio.lib()
+    L.lph_write_log.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int32),
+                                C.c_int, C.POINTER(C.c_float), C.c_int64]
+    g = np.ascontiguousarray(grid, np.float32)
+    calls = [("SurfRxy.txt", 0, cp.GetSFTImage(0)), ("SurfRxy.txt", 1, cp.GetRTdImage(0)),
+             ("SurfRxy.txt", 2, cp.GetRTdImage(0)), ("SurfRxy.txt", 3, cp.GetRTdImage(0)),
+             ("TransRxy.txt", 2, cp.GetRTdImage(2)), ("TransRxy.txt", 3, cp.GetRTdImage(2)),
+             ("FetalRxy.txt", 2, cp.GetRTdImage(1)), ("FetalRxy.txt", 3, cp.GetRTdImage(1)),
+             ("FluencePrz.txt", 4, cp.GetPhirzImage())]
+    for fname, kind, img in calls:
+        v = np.ascontiguousarray(img.data, np.float32)
+        e = np.array(img.extent, np.int32)
+        assert L.lph_write_log((d + "/").encode(), fname.encode(), kind, v.ctypes.data_as(C.POINTER(C.c_float)),
+                               e.ctypes.data_as(C.POINTER(C.c_int32)), v.shape[2],
+                               g.ctypes.data_as(C.POINTER(C.c_float)), photons) == 0
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_cpp_and_python_launchers_write_the_same_logs(tmp_path, name):
+    """lpsim (C++ launcher) and the Python launcher on the model's files, same seed: the
+    reference-format logs written from their GPU images are identical files."""
+    n = PHOTONS[name]
+    z, cfg = write_model(name, str(tmp_path), n)
+    w = modelio.load_model(cfg)
+    tri, _, med = arrays(z)
+    assert np.array_equal(w.tri.view(np.uint32), tri.view(np.uint32)) and np.array_equal(w.med, med)
+    for k in ("p_start", "v_start", "ep0xyz", "dimensions", "det_grid"):
+        assert np.array_equal(getattr(w, k).view(np.uint32), z[k].view(np.uint32)), k
+    out_c, out_p = tmp_path / "cpp", tmp_path / "py"
+    out_c.mkdir()
+    out_p.mkdir()
+    r = subprocess.run([modelio.LPSIM, "-f", cfg, "-s", "-a", "-o", str(out_c), "--seed", str(SEED)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "Writing Done." in r.stdout
+    cp = python_launcher(w, n, SEED, exact=False)
+    write_logs(cp, str(out_p), w.det_grid, n)
+    files = sorted(os.listdir(out_c))
+    assert files and files == sorted(os.listdir(out_p)), (files, sorted(os.listdir(out_p)))
+    for f in files:
+        assert filecmp.cmp(out_c / f, out_p / f, shallow=False), f
+    assert cp.GetSFTImage().data[:, :, 0].sum() > 0
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_launcher_images_match_the_oracle_with_common_random_numbers(tmp_path, name):
+    """Reference-order arithmetic on the GPU and the oracle consume the same Philox
+    numbers photon by photon; the images agree except for the few photons whose
+    trajectories part after a last-place difference flips a decision."""
+    n = min(PHOTONS[name], 20000)
+    _, cfg = write_model(name, str(tmp_path), n)
+    w = modelio.load_model(cfg)
+    cp = python_launcher(w, n, SEED, exact=True)
+    t = cp.GetTallies()
+    case = po.Case(tri=w.tri, nrm=w.nrm, med=w.med, nmuasg=w.nmuasg, p_start=w.p_start, v_start=w.v_start,
+                   ep0xyz=w.ep0xyz, dimensions=w.dimensions, det_grid=w.det_grid, fetal_id=w.fetal_id,
+                   chance=w.chance, w_threshold=w.w_threshold, factor=w.factor)
+    if name == "model4_curved":
+        r = po.run64(case, n, seed=SEED, compat=po.COMPAT_ALL)
+    else:
+        r = po.run(case, n, rng_mode=po.RNG_PHILOX, seed=SEED, compat=po.COMPAT_ALL)
+    assert t["counters"]["photons"] == n
+    for k, o in (("sft", r.sft), ("rtd", r.rtd), ("rz", r.rz), ("region", r.region)):
+        a, b = t[k].astype(np.float64).sum(), o.astype(np.float64).sum()
+        assert abs(a - b) <= 0.02 * max(b, 1.0), (k, a, b)
+    # most image bins receive only photons whose trajectories agree: equal to the bit
+    nz = (t["sft"] > 0) | (r.sft > 0)
+    same = np.mean(t["sft"][nz] == r.sft[nz])
+    assert same > (0.5 if name == "model4_curved" else 0.7), same
+    # events per photon agree closely (the same trajectories, step for step)
+    for k in ("scatter", "boundary"):
+        assert abs(t["counters"][k] - r.counters[k]) <= 0.02 * r.counters[k], k

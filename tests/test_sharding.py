@@ -45,8 +45,10 @@ def _worker(rank, world, port, kind, n, first, out_dir):
         case, compat = _case(kind)
         f, k = sharding.photon_range(n, rank, world, first)
         part = po.run(case, k, first=f, compat=compat, seed=77, nthreads=1)
-        total = sharding.reduce_host_tallies(_as_dict(part))
-        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), f=f, k=k,
+        d = _as_dict(part)
+        d["grad"] = part.grad.ravel()            # FP64 differentiation sums, reduced as float64
+        total = sharding.reduce_host_tallies(d)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), f=f, k=k, grad=total["grad"],
                  counters=np.array([total["counters"][c] for c in sorted(total["counters"])], np.uint64),
                  **{key: total[key] for key in KEYS})
     finally:
@@ -87,7 +89,7 @@ def test_photon_range_partitions_exactly():
 
 
 @pytest.mark.parametrize("world,kind,n,first", [(2, "slab", 1501, 0), (3, "slab", 1000, 5000),
-                                                (2, "abdomen", 160, 17)])
+                                                (2, "abdomen", 800, 17)])
 def test_sharded_tallies_equal_one_rank(world, kind, n, first, tmp_path):
     outs = _spawn(world, kind, n, first, tmp_path)
     case, compat = _case(kind)
@@ -99,6 +101,10 @@ def test_sharded_tallies_equal_one_rank(world, kind, n, first, tmp_path):
         for key in KEYS:
             assert np.array_equal(o[key], getattr(full, key)), key
         assert np.array_equal(o["counters"], want_counters)
+        # floating-point sums: equal to rounding
+        assert np.allclose(o["grad"], full.grad.ravel(), rtol=1e-12, atol=0.0)
+    if kind == "abdomen":
+        assert full.det[:, 0].any() and full.grad.any()
     assert full.counters["photons"] == n
     assert full.region.sum() > 0
 
