@@ -3,11 +3,12 @@ transport kernel against the oracle's perturbation-MC sums (same photons, refere
 arithmetic), against central finite differences with common random numbers (production
 arithmetic, high statistics), and through the forward/backward API.
 
-Tolerances: derivatives agree with finite differences within 2% of their value or 4
-standard errors of the adjoint estimate, whichever is larger; sums over the same photons
-in reference arithmetic agree with the oracle within 4 standard errors (only photons whose
-float trajectories part contribute to the difference); transport tallies are bit-identical
-with differentiation on and off."""
+Tolerances: a derivative that the batches resolve (standard error of adjoint minus
+difference at most 0.5 % of its value) agrees with the finite difference within 2 %, any
+other within 4 standard errors; sums over the same photons in reference arithmetic agree
+with the oracle within 4 standard errors (only photons whose float trajectories part
+contribute to the difference); transport tallies are bit-identical with differentiation
+on and off."""
 import numpy as np
 import pytest
 
@@ -82,50 +83,67 @@ def test_gradient_sums_match_oracle(oracle_lib, case):
         assert not bad.any(), (key, np.argwhere(bad), g[key][bad], ora[bad], tol[bad])
 
 
-def test_adjoint_matches_central_differences():
-    """4e6 photons in 8 batches; per batch the adjoint derivative and the central
-    difference (+-1 %, same photon ids) of every tissue region's mua and mus for every
-    ring.  The batch-to-batch spread of (adjoint - difference) gives the standard error
-    of the comparison, which includes the finite difference's own noise."""
-    w = _slab()
-    nm = np.array(w.nmuasg, np.float32)
-    B, n, seed = 8, 500_000, 11
-    params = [(reg, col) for reg in (1, 2, 3) for col in (1, 2)]
-    adj = {p: [] for p in params}
-    fdv = {p: [] for p in params}
-    for b in range(B):
+def test_adjoint_matches_central_differences_all_120():
+    """All 120 derivatives of config 4 (5 tissue regions x 6 rings x (mua, mus) x 2
+    wavelengths, on the curved abdomen at 40,000 triangles): the adjoint sums of one
+    differentiated pass against central differences (+-1 %, common random numbers: the
+    same photon ids at both parameter values), B batches of n photons each
+    (LP_FD_PHOTONS, default 2e7 per evaluation).  The batch-to-batch spread of
+    (adjoint - difference) gives the standard error se of the comparison.
+
+    A derivative the rings resolve (se at most 0.5 % of its value) must agree within 2 %;
+    every other one within 4 se.  No derivative is passed by a wider bound."""
+    import os
+    total = int(float(os.environ.get("LP_FD_PHOTONS", "2e7")))
+    B = 10
+    n = total // B
+    seed = 11
+    report = []
+    resolved = compared = 0
+    for lam in (660, 940):
+        w = workloads.curved_abdomen(wavelength=lam, freq=20)
+        nm = np.array(w.nmuasg, np.float32)
+        params = [(reg, col) for reg in range(1, nm.shape[0]) for col in (1, 2)]
+        adj = {p: [] for p in params}
+        fdv = {p: [] for p in params}
         with Simulation(0) as s:
             w.apply(s, seed=seed)
             s.set_gradient(True)
 
-            def signal(m):
+            def signal(m, b):
                 s.set_media(m)
                 return s.forward(n, b * n)
 
-            signal(nm)
-            g = s.gradient()
-            for reg, col in params:
-                h = np.float32(0.01) * nm[reg, col]
-                m_p, m_m = nm.copy(), nm.copy()
-                m_p[reg, col] = nm[reg, col] + h
-                m_m[reg, col] = nm[reg, col] - h
-                fd = (signal(m_p) - signal(m_m)) / (np.float64(m_p[reg, col]) - np.float64(m_m[reg, col]))
-                adj[(reg, col)].append(g["d_mua" if col == 1 else "d_mus"][:, reg])
-                fdv[(reg, col)].append(fd)
-    resolved = 0
-    for p in params:
-        a, f = np.array(adj[p]), np.array(fdv[p])
-        d = a - f
-        se = d.std(0, ddof=1) / np.sqrt(B)
-        am, fm = a.mean(0), f.mean(0)
-        tol = np.maximum(0.02 * np.abs(fm), 4 * se)
-        print("region %d %s adjoint %s difference %s se %s" % (p[0], "mua" if p[1] == 1 else "mus",
-                                                            np.array2string(am, precision=6),
-                                                            np.array2string(fm, precision=6),
-                                                            np.array2string(se, precision=2)))
-        assert np.all(np.abs(am - fm) <= tol), (p, am, fm, se)
-        resolved += int(np.sum(4 * se <= 0.02 * np.abs(fm)))
-    assert resolved >= 1      # at least one derivative is resolved to better than 2 % here
+            for b in range(B):
+                signal(nm, b)
+                g = s.gradient()
+                for reg, col in params:
+                    h = np.float32(0.01) * nm[reg, col]
+                    m_p, m_m = nm.copy(), nm.copy()
+                    m_p[reg, col] = nm[reg, col] + h
+                    m_m[reg, col] = nm[reg, col] - h
+                    fd = (signal(m_p, b) - signal(m_m, b)) / (np.float64(m_p[reg, col]) - np.float64(m_m[reg, col]))
+                    adj[(reg, col)].append(g["d_mua" if col == 1 else "d_mus"][:, reg])
+                    fdv[(reg, col)].append(fd)
+        for p in params:
+            a, f = np.array(adj[p]), np.array(fdv[p])
+            se = (a - f).std(0, ddof=1) / np.sqrt(B)
+            am, fm = a.mean(0), f.mean(0)
+            for d in range(am.size):
+                compared += 1
+                res = se[d] <= 0.005 * abs(fm[d])
+                resolved += int(res)
+                report.append((lam, p[0], "mua" if p[1] == 1 else "mus", d, am[d], fm[d], se[d], res))
+                if res:
+                    assert abs(am[d] - fm[d]) <= 0.02 * abs(fm[d]), report[-1]
+                else:
+                    assert abs(am[d] - fm[d]) <= 4 * se[d] + 1e-300, report[-1]
+    for r in report:
+        print("%d nm region %d %s ring %d: adjoint %.6g difference %.6g se %.2g %s" %
+              (r[0], r[1], r[2], r[3], r[4], r[5], r[6], "resolved" if r[7] else ""))
+    print(f"{resolved} of {compared} derivatives resolved to 0.5 % (se) and within 2 %")
+    assert compared == 120
+    assert resolved >= 40, resolved
 
 
 def test_forward_backward_and_autograd():
