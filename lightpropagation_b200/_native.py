@@ -17,7 +17,8 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "ou
 COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL, COMPAT_ALL = 1, 2, 4, 7
 NCOUNTERS = 16
 COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped", "rz_drop",
-                 "vox_drop", "photons", "draws", "safe_skip", "bvh_query", "bad_input", "bounds"]
+                 "vox_drop", "photons", "draws", "safe_skip", "bvh_query", "bad_input", "bounds",
+                 "region_mismatch"]
 FIX_ONE = float(2 ** 32)
 
 _fp = C.POINTER(C.c_float)
@@ -112,6 +113,7 @@ _SIGS = {
     "lp_set_cell_lists": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_cell_margin": ([C.c_void_p, C.c_float], C.c_int),
     "lp_set_tally_aggregation": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_set_query_path": ([C.c_void_p, C.c_uint32], C.c_int),
     "lp_set_smem_budget": ([C.c_void_p, C.c_int32], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),

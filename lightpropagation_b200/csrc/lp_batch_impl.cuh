@@ -64,6 +64,7 @@ __device__ __forceinline__ void warp_load_slot(WarpSlot &S, const KParams *inst,
         M.n_nodes = S.P.n_nodes;
         M.n_tri = S.P.n_tri;
         M.dbg = S.P.counters ? S.P.counters + kBoundsCounter : nullptr;
+        M.tri_eps = S.P.tri_eps;
     }
     __syncwarp();
 }

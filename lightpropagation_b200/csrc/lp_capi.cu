@@ -248,10 +248,11 @@ struct lp_ctx {
     DevBuf<uint32_t> cell_word;
     DevBuf<int32_t> cell_refs;
     int64_t n_cell_refs = 0;
-    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0, g_step_eps = 0;
+    float g_origin[3] = {0, 0, 0}, g_h = 0, g_unit = 0, g_eps = 0, g_step_eps = 0, g_push = 0;
     // lists hold the triangles touching each cell widened by cell_margin cells on every side
     float cell_margin = 0.5f;
     bool agg_tallies = false;   // lp_set_tally_aggregation
+    uint32_t query_path = 7u;   // lp_set_query_path (kQueryCarry | kQueryPrefetch | kQueryOneList)
     int32_t g_n[3] = {0, 0, 0};
     float grid_ms = 0;
     // differentiation (lp_set_gradient / lp_forward / lp_backward)
@@ -556,7 +557,10 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.g_h = c->g_h;
     P.g_margin = c->cell_margin * c->g_h;
     P.step_eps = c->g_step_eps;
+    P.boundary_push = c->exact ? 0.0f : c->g_push;
+    P.tri_eps = c->exact ? 0.0f : 2e-6f;
     P.agg_tallies = c->agg_tallies ? 1 : 0;
+    P.query_path = c->query_path;
 }
 
 // Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
@@ -797,6 +801,14 @@ int lp_set_mesh(lp_ctx *c, int64_t n_tri, const float *tri, const float *nrm, co
         c->tri_attr[i] = make_float4(v[0], v[1], v[2], fb);
     }
     c->n_tri = n_tri;
+    {
+        // boundary push of the production arithmetic: about 8 float ulps of the largest
+        // coordinate of the mesh (2^-23 = 1.19e-7)
+        double scale = 0.0;
+        for (int a = 0; a < 3; ++a)
+            scale = std::max({scale, std::fabs((double)c->bvh.lo[a]), std::fabs((double)c->bvh.hi[a])});
+        c->g_push = (float)(1e-6 * scale);
+    }
     c->max_region = 0;
     for (int64_t i = 0; i < 2 * n_tri; ++i) c->max_region = std::max(c->max_region, med[i]);
     c->have_mesh = true;
@@ -902,6 +914,14 @@ int lp_set_arithmetic(lp_ctx *c, int exact)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_arithmetic: ctx is NULL");
     c->exact = exact != 0;
+    return LP_OK;
+}
+
+int lp_set_query_path(lp_ctx *c, uint32_t flags)
+{
+    if (!c) return LP_ERR_INVALID;
+    if (flags > 7u) return fail(c, LP_ERR_INVALID, "lp_set_query_path: flags %u", flags);
+    c->query_path = flags;
     return LP_OK;
 }
 
@@ -1339,6 +1359,7 @@ int lp_query_triangles(lp_ctx *c, int64_t n, const float *orig, const float *dir
     smem_plan(c, c->smem_budget, nodes_smem, tris_smem);
     KParams P;
     fill_params(c, P, 0, 0, nodes_smem, tris_smem);
+    P.tri_eps = 0.0f;   // the reference's test: these queries are checked against its scan
     const int smem = lp::smem_bytes(nodes_smem, tris_smem);
     LP_CUDA(c, lp::launch_query(P, smem, n, o.p, d.p, rf.p, tm.p, io.p, to.p, s));
     LP_CUDA(c, cudaMemcpyAsync(id_out, io.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));

@@ -87,8 +87,13 @@ struct KParams {
     // a cell's list holds every triangle touching the cell widened by g_margin + g_eps on
     // every side; g_h is the cell edge; step_eps bounds the rounding of one position update
     float g_margin, g_h, step_eps;
+    // production arithmetic: distance a photon is moved off a face after a boundary event,
+    // and the barycentric tolerance of the hit test (both 0 in the reference arithmetic)
+    float boundary_push, tri_eps;
     // 1: absorption deposits are summed per cell across the warp before the atomic adds
     int32_t agg_tallies;
+    // query path switches (kQuery*), none of which changes a result
+    uint32_t query_path;
     // scratch: photon work counter
     unsigned long long *work;
 };
@@ -117,6 +122,21 @@ __device__ __forceinline__ bool in_range_dbg(unsigned long long *dbg, long long 
 #define LP_IN_RANGE(dbg, i, n) ::lp::in_range_dbg((dbg), (long long)(i), (long long)(n))
 #else
 #define LP_IN_RANGE(dbg, i, n) true
+#endif
+
+// Query path switches (KParams::query_path):
+//   kQueryCarry     carry the distance bound from step to step (less the steps taken);
+//                   without it every step starts from its cell's bound alone
+//   kQueryPrefetch  read the cell word before the Philox rounds on every step; without it
+//                   only when the carried bound is used up
+//   kQueryOneList   answer a short step from its own cell's (widened) list, with a bound
+//                   from the listed triangles' planes; without it from the lists of all
+//                   cells the step's box overlaps
+constexpr uint32_t kQueryCarry = 1u, kQueryPrefetch = 2u, kQueryOneList = 4u;
+#ifdef LP_QUERY_PATH_FIXED
+#define LP_QPATH(P) (LP_QUERY_PATH_FIXED)
+#else
+#define LP_QPATH(P) ((P).query_path)
 #endif
 
 constexpr uint32_t kCellEmpty = 0x80000000u;
@@ -242,6 +262,10 @@ struct MeshView {
     const float4 *s_ta, *s_tb, *s_tc;
     int32_t nodes_smem, tris_smem;
     int32_t n_nodes, n_tri;          // array sizes for the debug build's bounds checks
+    // barycentric tolerance of the hit test: 0 is the reference's test; a few 1e-6 (the
+    // production arithmetic) lets neighbouring triangles overlap along their shared
+    // edges, so no ray slips through the float gap between them
+    float tri_eps;
     unsigned long long *dbg;         // its counter of skipped accesses (may be null)
 };
 
@@ -269,12 +293,13 @@ __device__ __forceinline__ void test_tri(const MeshView &M, int j, V3 p, V3 v, i
     // with a relative margin far above the rounding of the divided values).  Only
     // candidates that pass pay for the three IEEE divisions of the reference test.
     const float aw = fabsf(w);
-    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= 0.0f && l >= 0.0f) : (t < 0.0f && k <= 0.0f && l <= 0.0f);
-    if (!sgn || fabsf(k) + fabsf(l) > aw * 1.0001f || fabsf(t) > best * aw * 1.0001f) return;
+    const float ek = M.tri_eps * aw;
+    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= -ek && l >= -ek) : (t < 0.0f && k <= ek && l <= ek);
+    if (!sgn || fabsf(k) + fabsf(l) > aw * (1.0001f + 3.0f * M.tri_eps) || fabsf(t) > best * aw * 1.0001f) return;
     t = t / w;
     k = k / w;
     l = l / w;
-    if (t > 0.0f && t < kNoHit && k >= 0.0f && l >= 0.0f && (k + l) < 1.0f &&
+    if (t > 0.0f && t < kNoHit && k >= -M.tri_eps && l >= -M.tri_eps && (k + l) < 1.0f + M.tri_eps &&
         (t < best || (t == best && o < bid))) {
         best = t;
         bid = o;
@@ -310,12 +335,13 @@ __device__ __forceinline__ void test_tri_safe(const MeshView &M, int j, V3 p, V3
     float k = dot3(VF, G);
     float l = dot3(GE, v);
     const float aw = fabsf(w);
-    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= 0.0f && l >= 0.0f) : (t < 0.0f && k <= 0.0f && l <= 0.0f);
-    if (!sgn || fabsf(k) + fabsf(l) > aw * 1.0001f || fabsf(t) > best * aw * 1.0001f) return;
+    const float ek = M.tri_eps * aw;
+    const bool sgn = (w > 0.0f) ? (t > 0.0f && k >= -ek && l >= -ek) : (t < 0.0f && k <= ek && l <= ek);
+    if (!sgn || fabsf(k) + fabsf(l) > aw * (1.0001f + 3.0f * M.tri_eps) || fabsf(t) > best * aw * 1.0001f) return;
     t = t / w;
     k = k / w;
     l = l / w;
-    if (t > 0.0f && t < kNoHit && k >= 0.0f && l >= 0.0f && (k + l) < 1.0f &&
+    if (t > 0.0f && t < kNoHit && k >= -M.tri_eps && l >= -M.tri_eps && (k + l) < 1.0f + M.tri_eps &&
         (t < best || (t == best && o < bid))) {
         best = t;
         bid = o;
@@ -324,7 +350,7 @@ __device__ __forceinline__ void test_tri_safe(const MeshView &M, int j, V3 p, V3
 
 // STACK: traversal stack entries; the host only runs a tree whose depth is below it.
 template <int STACK = kStackDepth>
-__device__ __forceinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
+__device__ __noinline__ int query_nearest(const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
                                              float &t_out)
 {
     float best = fminf(bound, kNoHit);

@@ -317,7 +317,8 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
 }
 
 // One iteration of the reference's do-while loop.  Returns false when the photon ends.
-template <bool Exact, bool Grad, int STACK = kStackDepth>
+// Agg: absorption deposits summed per cell across the warp before the atomic adds.
+template <bool Exact, bool Grad, int STACK = kStackDepth, bool Agg = false>
 __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
                                             unsigned long long *s_region, unsigned long long *s_cnt,
                                             Photon &ph, Counters &cnt, GradAcc *ga)
@@ -325,7 +326,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     // With no distance bound left (after a boundary, or once the steps have used it up)
     // the step surely needs the cell word: its load is issued before the Philox rounds so
     // that they hide its latency.  Otherwise it is read only if the step exceeds the bound.
-    const bool fresh = !(ph.safe > 0.0f);
+    const bool fresh = !(ph.safe > 0.0f) || (LP_QPATH(P) & kQueryPrefetch);
     uint32_t word = fresh ? cell_at(P, ph.px, ph.py, ph.pz) : 0u;
     EventRng rng;
     rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
@@ -347,6 +348,12 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     }
     float thit;
     int tri;
+    // reach: the production arithmetic also takes a face that lies up to a few rounding
+    // units beyond the step as the step's boundary.  A hit computed just past the step
+    // although it lies just within it would otherwise let the photon end its step on the
+    // far side of the face, outside the region it is labelled with.  The photon then stops
+    // on the face (and is moved off it, see below) with no residual step.
+    const float reach = Exact ? step : step + P.boundary_push + 1e-6f * step;
     // safe_here: lower bound of the distance from p to every triangle.  A step shorter
     // than it cannot reach one, so its bounded query would return "no hit" and is skipped;
     // after the step the bound shrinks by the step (plus the rounding of the move).
@@ -356,7 +363,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         tri = query_nearest<STACK>(M, p, v, ph.refTri, kNoHit, thit);
         cnt.query++;
         cnt.bvh++;
-    } else if (step < safe_here) {
+    } else if (reach < safe_here) {
         tri = -1;
         thit = kNoHit;
         cnt.skip++;
@@ -366,29 +373,29 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         if (word & kCellEmpty) {
             // a cell no triangle touches: its word holds a bound for all its points
             safe_here = safe_distance(P, word);
-            if (step < safe_here) {
+            if (reach < safe_here) {
                 tri = -1;
                 thit = kNoHit;
                 cnt.skip++;
                 done = true;
             }
-        } else if (P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
+        } else if ((LP_QPATH(P) & kQueryOneList) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
             // the cell's own list: a bound from the planes of its triangles, and the
             // query itself when the step stays inside the widened cell
-            done = list_query(P, M, p, v, ph.refTri, step, word, thit, tri, safe_here);
+            done = list_query(P, M, p, v, ph.refTri, reach, word, thit, tri, safe_here);
             if (done) cnt.query++;
         } else {
             safe_here = 0.0f;
         }
         if (!done) {
             bool used_bvh;
-            tri = cell_query<STACK>(P, M, p, v, ph.refTri, step, thit, used_bvh);
+            tri = cell_query<STACK>(P, M, p, v, ph.refTri, reach, thit, used_bvh);
             cnt.query++;
             cnt.bvh += used_bvh ? 1u : 0u;
         }
     }
     if (m.ambient) step = thit;
-    const bool boundary = (tri >= 0) ? (thit <= step) : (kNoHit <= step);
+    const bool boundary = (tri >= 0) ? (thit <= (m.ambient ? step : reach)) : (kNoHit <= step);
     if (boundary) {
         cnt.boundary++;
         ph.safe = 0.0f;
@@ -407,6 +414,9 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             const int inner = ids & 0xffff, outer = ids >> 16;
             V3 nv = v3(at.x, at.y, at.z);
             int nxt_id = (ph.curr == outer) ? inner : outer;
+            // a photon whose region is neither side of the face it meets has passed through
+            // another face unseen (a crack between triangles that the float test leaves)
+            if (ph.curr != inner && ph.curr != outer) atomicAdd(s_cnt + 14, 1ull);
             if (!LP_IN_RANGE(dbg, nxt_id, P.n_media)) nxt_id = ph.curr;
             const Medium nx = s_media[nxt_id];
             if (P.compat & 0x2u) {
@@ -465,6 +475,22 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
                 musNew = m.mus;
             }
             ph.vx = vout.x; ph.vy = vout.y; ph.vz = vout.z;
+            if (!Exact) {
+                // The hit point lies on the face's plane only to float rounding, on either
+                // side.  On the wrong side, the next segment can cross a neighbouring face of
+                // the same surface a rounding distance away (the face itself is excluded by
+                // refTri): a spurious second boundary event, which in float happens to about
+                // 2e-4 of the photons of a curved mesh and lets them leave the region they
+                // are labelled with.  The production arithmetic moves the photon off the
+                // plane, to the side it travels to, by a few rounding units of the scene's
+                // coordinates and of the distance travelled.  (The reference-order
+                // arithmetic keeps the reference's behaviour.)
+                const float push = P.boundary_push + 1e-6f * thit;
+                const float sp = (dot3(vout, nv) > 0.0f) ? push : -push;
+                ph.px = __fmaf_rn(sp, nv.x, ph.px);
+                ph.py = __fmaf_rn(sp, nv.y, ph.py);
+                ph.pz = __fmaf_rn(sp, nv.z, ph.pz);
+            }
             if (muaNew == 0.0f || musNew == 0.0f) {
                 const float dist = fabsf(dot3(v3(P.nzx, P.nzy, P.nzz),
                                               v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz)));
@@ -479,7 +505,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             ph.curr = newID;
             ph.refTri = tri;
             if (newID == P.fetal_id) ph.flags |= F_FETAL;
-            ph.unfin = (step - thit) * m.mut;
+            ph.unfin = Exact ? (step - thit) * m.mut : fmaxf(step - thit, 0.0f) * m.mut;
             if (newID != prev) {
                 if (ph.region_acc) atomicAdd(s_region + prev, ph.region_acc);
                 ph.region_acc = 0;
@@ -501,7 +527,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.py = ph.py + step * ph.vy;
         ph.pz = ph.pz + step * ph.vz;
         ph.refTri = -1;
-        ph.safe = fmaxf(safe_here - step - P.step_eps, 0.0f);
+        ph.safe = (LP_QPATH(P) & kQueryCarry) ? fmaxf(safe_here - step - P.step_eps, 0.0f) : 0.0f;
         if (Grad) {
             ph.seg_len += step;
             ph.seg_k++;
@@ -550,7 +576,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         }
         if (!rz_in) cnt.rz_drop++;
         const int rz_key = rz_in ? row * P.rz_nr + col : -1;
-        if (P.agg_tallies) {
+        if (Agg) {
             // warp-aggregated deposits: the lanes of this branch that hit the same cell
             // are matched, their fixed-point values summed exactly, and one leader per
             // cell issues the atomic add (integer sums: same tallies as the plain form)
@@ -563,6 +589,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
                     unsigned long long *c = P.rz + 2 * (int64_t)rz_key;
                     if (a) atomicAdd(c, a);
                     if (b) atomicAdd(c + 1, b);
+                    atomicAdd(s_cnt + 15, 1ull);   // leaders: 1 - leaders / deposits is the match rate
                 }
             }
             const unsigned g_vox = __match_any_sync(act, vox_key);
@@ -645,10 +672,11 @@ __device__ __forceinline__ MeshView stage_mesh(const KParams &P, unsigned char *
     M.n_nodes = P.n_nodes;
     M.n_tri = P.n_tri;
     M.dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
+    M.tri_eps = P.tri_eps;
     return M;
 }
 
-template <bool Exact, bool Grad>
+template <bool Exact, bool Grad, bool Agg = false>
 __global__ void __launch_bounds__(kBlock, LP_TRANSPORT_MIN_BLOCKS) transport_kernel(const __grid_constant__ KParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -696,7 +724,7 @@ __global__ void __launch_bounds__(kBlock, LP_TRANSPORT_MIN_BLOCKS) transport_ker
         }
         if (!__any_sync(0xffffffffu, alive)) break;
         if (alive) {
-            if (!step_photon<Exact, Grad>(P, M, s_media, s_region, s_cnt, ph, cnt, &ga)) {
+            if (!step_photon<Exact, Grad, kStackDepth, Agg>(P, M, s_media, s_region, s_cnt, ph, cnt, &ga)) {
                 if (ph.region_acc) atomicAdd(s_region + ph.curr, ph.region_acc);
                 if (Grad) {
                     ga.L[ph.curr] += ph.seg_len;
@@ -735,11 +763,21 @@ __global__ void __launch_bounds__(kBlock, LP_TRANSPORT_MIN_BLOCKS) transport_ker
 }
 
 // P.grad selects the differentiating instantiation.
+// The warp-aggregated form exists for the production arithmetic without differentiation
+// only (P.agg_tallies is ignored otherwise).
 template <bool Exact>
 cudaError_t launch_transport_t(const KParams &P, int grid, int smem, cudaStream_t s)
 {
-    if (P.grad) transport_kernel<Exact, true><<<grid, kBlock, smem, s>>>(P);
-    else transport_kernel<Exact, false><<<grid, kBlock, smem, s>>>(P);
+    if (!Exact && !P.grad && P.agg_tallies) {
+        cudaError_t e = cudaFuncSetAttribute(transport_kernel<false, false, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        transport_kernel<false, false, true><<<grid, kBlock, smem, s>>>(P);
+    } else if (P.grad) {
+        transport_kernel<Exact, true><<<grid, kBlock, smem, s>>>(P);
+    } else {
+        transport_kernel<Exact, false><<<grid, kBlock, smem, s>>>(P);
+    }
     return cudaGetLastError();
 }
 

@@ -582,6 +582,7 @@ static void trace_photon(const ctx_t *C, rng_t *R, int64_t pid, lpo_tallies *T, 
             } else {
                 if (track) L[curr] += ph.steptoboundary;
                 int inner = P->med[2 * triID], outer = P->med[2 * triID + 1];
+                if (curr != inner && curr != outer) T->counters[LPO_C_MISMATCH]++;
                 nv = normalize(ld3(P->nrm, triID));
                 const float *nxt = (curr == outer) ? nm + 4 * inner : nm + 4 * outer;
                 if (P->compat & LPO_COMPAT_AXIS_NORMAL) {

@@ -60,6 +60,7 @@ enum {
     LPO_C_VOX_DROP,     /* absorption deposits outside the voxel grid             */
     LPO_C_PHOTONS,      /* photons traced                                         */
     LPO_C_DRAWS,        /* uniform numbers consumed                               */
+    LPO_C_MISMATCH,     /* boundary events on a face that does not border the photon's region */
     LPO_NCOUNTERS = 16
 };
 

@@ -537,6 +537,7 @@ static void trace64(const ctx64_t *C, rng64_t *R, int64_t pid, lpo_tallies *T, f
             } else {
                 if (track) L[curr] += thit;
                 int inner = P->med[2 * tri], outer = P->med[2 * tri + 1];
+                if (curr != inner && curr != outer) T->counters[LPO_C_MISMATCH]++;
                 nv = normalize(ldf3(P->nrm, tri));
                 const float *nxt = (curr == outer) ? nm + 4 * inner : nm + 4 * outer;
                 if (P->compat & LPO_COMPAT_AXIS_NORMAL) {

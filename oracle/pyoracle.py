@@ -25,7 +25,7 @@ COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL = 1, 2, 4
 COMPAT_ALL = 7
 NCOUNTERS = 16
 COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped",
-                 "rz_drop", "vox_drop", "photons", "draws"]
+                 "rz_drop", "vox_drop", "photons", "draws", "region_mismatch"]
 FIX_SCALE = float(2 ** 32)
 
 _fp = C.POINTER(C.c_float)

@@ -31,7 +31,7 @@ FIX = 2.0 ** 32
 #   [alpha, r, comp] for rtd, [z, r, comp] for rz, [z, y, x] for vox); "vox_l2" is the
 #   resolution of the voxel relative-L2 comparison.
 SPEC = {
-    "plain_slab": dict(workload=("plain_slab", {}), n=200_000, B=20, seed=0x64_0001,
+    "plain_slab": dict(workload=("plain_slab", {}), n=500_000, B=20, seed=0x64_0011,
                        blocks={"sft": (1, 1, 1), "rtd": (1, 1, 1), "rz": (1, 1, 1), "vox": (3, 5, 5),
                                "vox_l2": (1, 1, 1)}),
     "abdomen660": dict(workload=("curved_abdomen", {"wavelength": 660, "freq": 12}), n=200_000, B=20,

@@ -150,9 +150,12 @@ def test_launcher_images_match_the_oracle_with_common_random_numbers(tmp_path, n
         a, b = t[k].astype(np.float64).sum(), o.astype(np.float64).sum()
         assert abs(a - b) <= 0.02 * max(b, 1.0), (k, a, b)
     # most image bins receive only photons whose trajectories agree: equal to the bit
+    # against the FP32 oracle; against the FP64 oracle (whose weights differ from the
+    # float ones in the last bits) equal to 1e-4
     nz = (t["sft"] > 0) | (r.sft > 0)
-    same = np.mean(t["sft"][nz] == r.sft[nz])
-    assert same > (0.5 if name == "model4_curved" else 0.7), same
+    a, b = t["sft"][nz].astype(np.float64), r.sft[nz].astype(np.float64)
+    same = np.mean(np.abs(a - b) <= 1e-4 * np.maximum(a, b)) if name == "model4_curved" else np.mean(a == b)
+    assert same > 0.7, same
     # events per photon agree closely (the same trajectories, step for step)
     for k in ("scatter", "boundary"):
         assert abs(t["counters"][k] - r.counters[k]) <= 0.02 * r.counters[k], k

@@ -164,7 +164,8 @@ def test_run_sharded_over_nccl_on_one_rank():
         dist.destroy_process_group()
     for key in KEYS + ("counters",):
         assert np.array_equal(got[key], want[key]), key
-    assert np.array_equal(got["grad"], want["grad"])
+    # FP64 atomic sums: their order, and so their last bits, vary from run to run
+    assert np.allclose(got["grad"], want["grad"], rtol=1e-12, atol=0.0)
 
 
 _DEBUG_CHILD = r"""

@@ -86,9 +86,12 @@ def batch_z(a, b):
         return np.where(se2 > 0, (a.mean(0) - b.mean(0)) / np.sqrt(se2), 0.0)
 
 
-def image_z(g, o, key, min_rel_se=0.3):
+def image_z(g, o, key, min_rel_se=0.1):
     """Per-bin z over the bins that both sides resolve (relative standard error of the
-    mean below min_rel_se on each side)."""
+    mean below min_rel_se on each side).  A bin fed by a handful of heavy photons (the
+    transmitted and fetal components far from the source) has a skewed batch
+    distribution whose sample variance understates the error of its mean; 10 % keeps
+    those out."""
     mg, vg, mo, vo = g[key + "_mean"], g[key + "_var"], o[key + "_mean"], o[key + "_var"]
     ok = (mo > 0) & (mg > 0) & (vo > 0) & (vg > 0)
     ok &= (np.sqrt(vo) < min_rel_se * mo) & (np.sqrt(vg) < min_rel_se * mg)
@@ -136,12 +139,12 @@ def slab_pair():
     o = fx.load("plain_slab")
     w = fx.workload("plain_slab")
     assert fx.mesh_hash(w) == str(o["mesh_hash"]), "the workload changed since the fixture was made"
-    g = gpu_batches(w, fx.SPEC["plain_slab"], 10_000_000, 10, seed=0x5EED)
+    g = gpu_batches(w, fx.SPEC["plain_slab"], 5_000_000, 20, seed=0x5EED)
     return g, o, w
 
 
 def test_slab_scalar_tallies_vs_fp64_oracle(slab_pair):
-    """1e8 production photons on the plain slab (config 1) against 4e6 FP64-oracle photons:
+    """1e8 production photons on the plain slab (config 1) against 1e7 FP64-oracle photons:
     surface, fetal and transmitted weight and absorption per region, |z| < 3 each."""
     g, o, _ = slab_pair
     z = batch_z(g["scalars_b"], o["scalars_b"])
