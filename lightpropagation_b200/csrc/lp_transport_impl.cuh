@@ -316,12 +316,165 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
     ph.safe = 0.0f;
 }
 
-// One iteration of the reference's do-while loop.  Returns false when the photon ends.
-// Agg: absorption deposits summed per cell across the warp before the atomic adds.
-template <bool Exact, bool Grad, int STACK = kStackDepth, bool Agg = false>
-__device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
-                                            unsigned long long *s_region, unsigned long long *s_cnt,
-                                            Photon &ph, Counters &cnt, GradAcc *ga)
+// A boundary event (.cl:1443-1465 with TransmitOrReflect, .cl:921-1018): the photon moves
+// thit to the face `tri` (-1: no face, it leaves the model), then is transmitted or
+// reflected with probability from the Fresnel equations (xi against R).  Out of line: it
+// runs about once per hundred steps, and keeping its code out of the step loop keeps the
+// loop's instructions in cache for the warps that scatter.
+template <bool Exact, bool Grad>
+static __device__ __noinline__ void boundary_event(const KParams &P, const Medium *s_media,
+                                                       unsigned long long *s_region, unsigned long long *s_cnt,
+                                                       Photon &ph, GradAcc *ga, int tri, float thit, float step,
+                                                       float xi)
+{
+    [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
+    const Medium m = s_media[ph.curr];
+    const V3 v = v3(ph.vx, ph.vy, ph.vz);
+    ph.safe = 0.0f;
+    ph.px = ph.px + thit * ph.vx;
+    ph.py = ph.py + thit * ph.vy;
+    ph.pz = ph.pz + thit * ph.vz;
+    ph.refTri = -1;
+    if (tri < 0) {
+        // the reference would read mediumIDs[-1] here; the photon leaves the model
+        atomicAdd(s_cnt + 4, 1ull);
+        ph.w = 0.0f;
+    } else if (LP_IN_RANGE(dbg, tri, P.n_tri)) {
+        const float4 at = __ldg(P.tri_attr + tri);
+        const int ids = __float_as_int(at.w);
+        const int inner = ids & 0xffff, outer = ids >> 16;
+        V3 nv = v3(at.x, at.y, at.z);
+        int nxt_id = (ph.curr == outer) ? inner : outer;
+        // a photon whose region is neither side of the face it meets has passed through
+        // another face unseen (a crack between triangles that the float test leaves)
+        if (ph.curr != inner && ph.curr != outer) atomicAdd(s_cnt + 14, 1ull);
+        if (!LP_IN_RANGE(dbg, nxt_id, P.n_media)) nxt_id = ph.curr;
+        const Medium nx = s_media[nxt_id];
+        if (P.compat & 0x2u) {
+            if (fabsf(sqrtf(ph.px * ph.px + ph.py * ph.py)) < 0.01f) {
+                const float sg = sign_cl(dot3(nv, v3(P.ezx, P.ezy, P.ezz)));
+                nv = scl3(sg, v3(P.nzx, P.nzy, P.nzz));
+            }
+        }
+        ph.nvx = nv.x; ph.nvy = nv.y; ph.nvz = nv.z;
+        // TransmitOrReflect (.cl:921-1018)
+        const float cosIn = dot3(nv, v);
+        const float absCosIn = fabsf(cosIn);
+        const float n1 = m.n, n2 = nx.n;
+        float cos_crit = 0.0f;
+        if (n1 > n2) cos_crit = sqrtf(1.0f - (n2 / n1) * (n2 / n1));
+        float r;
+        if (absCosIn <= cos_crit) r = 1.0f;
+        else r = fresnel(n1, n2, (P.compat & 0x4u) ? cosIn : absCosIn);
+        int newID;
+        float muaNew, musNew;
+        V3 vout;
+        if (Exact) {
+            const V3 e_y = norm3(cross3(nv, cross3(nv, v)));
+            if (xi > r) {
+                const float sinT = sqrtf(1.0f - cosIn * cosIn) * n1 / n2;
+                float cosT = -sqrtf(1.0f - sinT * sinT);
+                if (cosIn > 0.0f) cosT = fabsf(cosT);
+                vout = norm3(sub3(scl3(cosT, nv), scl3(sinT, e_y)));
+            } else {
+                const float sinR = sqrtf(1.0f - cosIn * cosIn);
+                const V3 t = norm3(add3(scl3(cosIn, nv), scl3(sinR, e_y)));
+                vout = v3(-t.x, -t.y, -t.z);
+            }
+        } else {
+            if (xi > r) {
+                // v' = cosT n - sinT e_y with e_y = (n cosIn - v) / sinIn (unit n, v)
+                const float s2 = fmaxf(0.0f, 1.0f - cosIn * cosIn);
+                const float sinT = sqrtf(s2) * __fdividef(n1, n2);
+                float cosT = sqrtf(fmaxf(0.0f, 1.0f - sinT * sinT));
+                if (!(cosIn > 0.0f)) cosT = -cosT;
+                const float k = s2 > 1e-12f ? sinT * rsqrtf(s2) : 0.0f;
+                vout = fast_norm(v3(cosT * nv.x - k * (nv.x * cosIn - v.x), cosT * nv.y - k * (nv.y * cosIn - v.y),
+                                    cosT * nv.z - k * (nv.z * cosIn - v.z)));
+            } else {
+                vout = fast_norm(v3(v.x - 2.0f * cosIn * nv.x, v.y - 2.0f * cosIn * nv.y,
+                                    v.z - 2.0f * cosIn * nv.z));
+            }
+        }
+        if (xi > r) {
+            newID = (cosIn > 0.0f) ? outer : inner;
+            muaNew = nx.mua;
+            musNew = nx.mus;
+        } else {
+            newID = ph.curr;
+            muaNew = m.mua;
+            musNew = m.mus;
+        }
+        ph.vx = vout.x; ph.vy = vout.y; ph.vz = vout.z;
+        if (!Exact) {
+            // The hit point lies on the face's plane only to float rounding, on either
+            // side.  On the wrong side, the next segment can cross a neighbouring face of
+            // the same surface a rounding distance away (the face itself is excluded by
+            // refTri): a spurious second boundary event, which in float happens to about
+            // 2e-4 of the photons of a curved mesh and lets them leave the region they
+            // are labelled with.  The production arithmetic moves the photon off the
+            // plane, to the side it travels to, by a few rounding units of the scene's
+            // coordinates and of the distance travelled.  (The reference-order
+            // arithmetic keeps the reference's behaviour.)
+            const float push = P.boundary_push + 1e-6f * thit;
+            const float sp = (dot3(vout, nv) > 0.0f) ? push : -push;
+            ph.px = __fmaf_rn(sp, nv.x, ph.px);
+            ph.py = __fmaf_rn(sp, nv.y, ph.py);
+            ph.pz = __fmaf_rn(sp, nv.z, ph.pz);
+        }
+        if (muaNew == 0.0f || musNew == 0.0f) {
+            const float dist = fabsf(dot3(v3(P.nzx, P.nzy, P.nzz),
+                                          v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz)));
+            uint32_t kind;
+            if (dist > P.distMin) kind = EXIT_TRANS;
+            else kind = (ph.flags & F_FETAL) ? EXIT_SURF_FETAL : EXIT_SURF;
+            ph.exit_w = ph.w * P.exitScale;
+            ph.flags = (ph.flags & ~(3u << EXIT_SHIFT)) | (kind << EXIT_SHIFT);
+            ph.w = 0.0f;
+        }
+        const int prev = ph.curr;
+        ph.curr = newID;
+        ph.refTri = tri;
+        if (newID == P.fetal_id) ph.flags |= F_FETAL;
+        ph.unfin = Exact ? (step - thit) * m.mut : fmaxf(step - thit, 0.0f) * m.mut;
+        if (newID != prev) {
+            if (ph.region_acc) atomicAdd(s_region + prev, ph.region_acc);
+            ph.region_acc = 0;
+            if (Grad) {
+                ga->L[prev] += ph.seg_len + thit;
+                ga->k[prev] += ph.seg_k;
+                ph.seg_len = 0.0f;
+                ph.seg_k = 0;
+            }
+        } else if (Grad) {
+            ph.seg_len += thit;
+        }
+    } else {
+        ph.w = 0.0f;   // debug build: a triangle index out of range ends the photon
+    }
+}
+
+// A step in three parts: propose_step draws the event's random numbers and the step
+// length and decides whether the step can reach a triangle; query_step finds the nearest
+// triangle within reach; complete_step moves the photon (boundary event, or absorption and
+// scattering), scores it and plays roulette.  One call of each in turn is one iteration of
+// the reference's do-while loop (.cl:1388-1600).  (Letting the lanes whose step needs a
+// query wait until several of a warp do, and running their queries together, measured
+// slower on every batch size: the waiting lanes cost more steps per warp iteration than
+// the shared queries save.)
+struct Pending {
+    float step, reach, safe_here;   // step length, its reach, distance bound at the position
+    float u1, u2, u3;               // the event's uniforms after the step length's
+    uint32_t word;                  // cell word at the position
+};
+enum : int { kStepEnded = 0, kStepClear = 1, kStepQuery = 2 };
+
+// kStepQuery: the step may reach a triangle and needs a query; kStepClear: no triangle
+// lies within its reach (complete_step with tri = -1); kStepEnded: the photon ended
+// (debug build: a region id out of range).
+template <bool Exact>
+__device__ __forceinline__ int propose_step(const KParams &P, const Medium *s_media, Photon &ph, Counters &cnt,
+                                            Pending &pd)
 {
     // With no distance bound left (after a boundary, or once the steps have used it up)
     // the step surely needs the cell word: its load is issued before the Philox rounds so
@@ -333,7 +486,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
     if (!LP_IN_RANGE(dbg, ph.curr, P.n_media)) {
         ph.w = 0.0f;
-        return false;
+        return kStepEnded;
     }
     const Medium m = s_media[ph.curr];
     float step = 0.0f;
@@ -346,181 +499,91 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             ph.unfin = 0.0f;
         }
     }
-    float thit;
-    int tri;
+    pd.step = step;
     // reach: the production arithmetic also takes a face that lies up to a few rounding
     // units beyond the step as the step's boundary.  A hit computed just past the step
     // although it lies just within it would otherwise let the photon end its step on the
     // far side of the face, outside the region it is labelled with.  The photon then stops
-    // on the face (and is moved off it, see below) with no residual step.
+    // on the face (and is moved off it, see boundary_event) with no residual step.
     const float reach = Exact ? step : step + P.boundary_push + 1e-6f * step;
+    pd.reach = reach;
+    pd.u1 = rng.u1;
+    pd.u2 = rng.u2;
+    pd.u3 = rng.u3;
     // safe_here: lower bound of the distance from p to every triangle.  A step shorter
     // than it cannot reach one, so its bounded query would return "no hit" and is skipped;
     // after the step the bound shrinks by the step (plus the rounding of the move).
-    float safe_here = ph.safe;
+    pd.safe_here = ph.safe;
+    pd.word = word;
+    if (m.ambient) return kStepQuery;
+    if (reach < pd.safe_here) {
+        cnt.skip++;
+        return kStepClear;
+    }
+    if (!fresh) word = cell_at(P, ph.px, ph.py, ph.pz);
+    pd.word = word;
+    if (word & kCellEmpty) {
+        // a cell no triangle touches: its word holds a bound for all its points
+        pd.safe_here = safe_distance(P, word);
+        if (reach < pd.safe_here) {
+            cnt.skip++;
+            return kStepClear;
+        }
+    }
+    return kStepQuery;
+}
+
+// The nearest triangle within the step's reach (-1: none) and its distance thit; updates
+// the distance bound the query establishes.
+template <int STACK>
+__device__ __forceinline__ int query_step(const KParams &P, const MeshView &M, const Medium *s_media,
+                                          const Photon &ph, Counters &cnt, Pending &pd, float &thit)
+{
     const V3 p = v3(ph.px, ph.py, ph.pz), v = v3(ph.vx, ph.vy, ph.vz);
-    if (m.ambient) {
+    int tri = -1;
+    if (s_media[ph.curr].ambient) {
         tri = query_nearest<STACK>(M, p, v, ph.refTri, kNoHit, thit);
         cnt.query++;
         cnt.bvh++;
-    } else if (reach < safe_here) {
-        tri = -1;
-        thit = kNoHit;
-        cnt.skip++;
-    } else {
-        if (!fresh) word = cell_at(P, ph.px, ph.py, ph.pz);
-        bool done = false;
-        if (word & kCellEmpty) {
-            // a cell no triangle touches: its word holds a bound for all its points
-            safe_here = safe_distance(P, word);
-            if (reach < safe_here) {
-                tri = -1;
-                thit = kNoHit;
-                cnt.skip++;
-                done = true;
-            }
-        } else if ((LP_QPATH(P) & kQueryOneList) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
-            // the cell's own list: a bound from the planes of its triangles, and the
-            // query itself when the step stays inside the widened cell
-            done = list_query(P, M, p, v, ph.refTri, reach, word, thit, tri, safe_here);
-            if (done) cnt.query++;
-        } else {
-            safe_here = 0.0f;
-        }
-        if (!done) {
-            bool used_bvh;
-            tri = cell_query<STACK>(P, M, p, v, ph.refTri, reach, thit, used_bvh);
-            cnt.query++;
-            cnt.bvh += used_bvh ? 1u : 0u;
-        }
+        return tri;
     }
+    const uint32_t word = pd.word;
+    bool done = false;
+    if (word & kCellEmpty) {
+        // pd.safe_here holds the empty cell's bound, which the step exceeds
+    } else if ((LP_QPATH(P) & kQueryOneList) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
+        // the cell's own list: a bound from the planes of its triangles, and the
+        // query itself when the step stays inside the widened cell
+        done = list_query(P, M, p, v, ph.refTri, pd.reach, word, thit, tri, pd.safe_here);
+        if (done) cnt.query++;
+    } else {
+        pd.safe_here = 0.0f;
+    }
+    if (!done) {
+        bool used_bvh;
+        tri = cell_query<STACK>(P, M, p, v, ph.refTri, pd.reach, thit, used_bvh);
+        cnt.query++;
+        cnt.bvh += used_bvh ? 1u : 0u;
+    }
+    return tri;
+}
+
+// Returns false when the photon ends.  Agg: absorption deposits summed per cell across
+// the warp before the atomic adds.
+template <bool Exact, bool Grad, bool Agg = false>
+__device__ __forceinline__ bool complete_step(const KParams &P, const Medium *s_media, unsigned long long *s_region,
+                                              unsigned long long *s_cnt, Photon &ph, Counters &cnt, GradAcc *ga,
+                                              const Pending &pd, int tri, float thit)
+{
+    const Medium m = s_media[ph.curr];
+    const V3 v = v3(ph.vx, ph.vy, ph.vz);
+    float step = pd.step;
+    const float reach = pd.reach, safe_here = pd.safe_here;
     if (m.ambient) step = thit;
     const bool boundary = (tri >= 0) ? (thit <= (m.ambient ? step : reach)) : (kNoHit <= step);
     if (boundary) {
         cnt.boundary++;
-        ph.safe = 0.0f;
-        ph.px = ph.px + thit * ph.vx;
-        ph.py = ph.py + thit * ph.vy;
-        ph.pz = ph.pz + thit * ph.vz;
-        ph.refTri = -1;
-        const float xi = rng.u1;
-        if (tri < 0) {
-            // the reference would read mediumIDs[-1] here; the photon leaves the model
-            atomicAdd(s_cnt + 4, 1ull);
-            ph.w = 0.0f;
-        } else if (LP_IN_RANGE(dbg, tri, P.n_tri)) {
-            const float4 at = __ldg(P.tri_attr + tri);
-            const int ids = __float_as_int(at.w);
-            const int inner = ids & 0xffff, outer = ids >> 16;
-            V3 nv = v3(at.x, at.y, at.z);
-            int nxt_id = (ph.curr == outer) ? inner : outer;
-            // a photon whose region is neither side of the face it meets has passed through
-            // another face unseen (a crack between triangles that the float test leaves)
-            if (ph.curr != inner && ph.curr != outer) atomicAdd(s_cnt + 14, 1ull);
-            if (!LP_IN_RANGE(dbg, nxt_id, P.n_media)) nxt_id = ph.curr;
-            const Medium nx = s_media[nxt_id];
-            if (P.compat & 0x2u) {
-                if (fabsf(sqrtf(ph.px * ph.px + ph.py * ph.py)) < 0.01f) {
-                    const float sg = sign_cl(dot3(nv, v3(P.ezx, P.ezy, P.ezz)));
-                    nv = scl3(sg, v3(P.nzx, P.nzy, P.nzz));
-                }
-            }
-            ph.nvx = nv.x; ph.nvy = nv.y; ph.nvz = nv.z;
-            // TransmitOrReflect (.cl:921-1018)
-            const float cosIn = dot3(nv, v);
-            const float absCosIn = fabsf(cosIn);
-            const float n1 = m.n, n2 = nx.n;
-            float cos_crit = 0.0f;
-            if (n1 > n2) cos_crit = sqrtf(1.0f - (n2 / n1) * (n2 / n1));
-            float r;
-            if (absCosIn <= cos_crit) r = 1.0f;
-            else r = fresnel(n1, n2, (P.compat & 0x4u) ? cosIn : absCosIn);
-            int newID;
-            float muaNew, musNew;
-            V3 vout;
-            if (Exact) {
-                const V3 e_y = norm3(cross3(nv, cross3(nv, v)));
-                if (xi > r) {
-                    const float sinT = sqrtf(1.0f - cosIn * cosIn) * n1 / n2;
-                    float cosT = -sqrtf(1.0f - sinT * sinT);
-                    if (cosIn > 0.0f) cosT = fabsf(cosT);
-                    vout = norm3(sub3(scl3(cosT, nv), scl3(sinT, e_y)));
-                } else {
-                    const float sinR = sqrtf(1.0f - cosIn * cosIn);
-                    const V3 t = norm3(add3(scl3(cosIn, nv), scl3(sinR, e_y)));
-                    vout = v3(-t.x, -t.y, -t.z);
-                }
-            } else {
-                if (xi > r) {
-                    // v' = cosT n - sinT e_y with e_y = (n cosIn - v) / sinIn (unit n, v)
-                    const float s2 = fmaxf(0.0f, 1.0f - cosIn * cosIn);
-                    const float sinT = sqrtf(s2) * __fdividef(n1, n2);
-                    float cosT = sqrtf(fmaxf(0.0f, 1.0f - sinT * sinT));
-                    if (!(cosIn > 0.0f)) cosT = -cosT;
-                    const float k = s2 > 1e-12f ? sinT * rsqrtf(s2) : 0.0f;
-                    vout = fast_norm(v3(cosT * nv.x - k * (nv.x * cosIn - v.x), cosT * nv.y - k * (nv.y * cosIn - v.y),
-                                        cosT * nv.z - k * (nv.z * cosIn - v.z)));
-                } else {
-                    vout = fast_norm(v3(v.x - 2.0f * cosIn * nv.x, v.y - 2.0f * cosIn * nv.y,
-                                        v.z - 2.0f * cosIn * nv.z));
-                }
-            }
-            if (xi > r) {
-                newID = (cosIn > 0.0f) ? outer : inner;
-                muaNew = nx.mua;
-                musNew = nx.mus;
-            } else {
-                newID = ph.curr;
-                muaNew = m.mua;
-                musNew = m.mus;
-            }
-            ph.vx = vout.x; ph.vy = vout.y; ph.vz = vout.z;
-            if (!Exact) {
-                // The hit point lies on the face's plane only to float rounding, on either
-                // side.  On the wrong side, the next segment can cross a neighbouring face of
-                // the same surface a rounding distance away (the face itself is excluded by
-                // refTri): a spurious second boundary event, which in float happens to about
-                // 2e-4 of the photons of a curved mesh and lets them leave the region they
-                // are labelled with.  The production arithmetic moves the photon off the
-                // plane, to the side it travels to, by a few rounding units of the scene's
-                // coordinates and of the distance travelled.  (The reference-order
-                // arithmetic keeps the reference's behaviour.)
-                const float push = P.boundary_push + 1e-6f * thit;
-                const float sp = (dot3(vout, nv) > 0.0f) ? push : -push;
-                ph.px = __fmaf_rn(sp, nv.x, ph.px);
-                ph.py = __fmaf_rn(sp, nv.y, ph.py);
-                ph.pz = __fmaf_rn(sp, nv.z, ph.pz);
-            }
-            if (muaNew == 0.0f || musNew == 0.0f) {
-                const float dist = fabsf(dot3(v3(P.nzx, P.nzy, P.nzz),
-                                              v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz)));
-                uint32_t kind;
-                if (dist > P.distMin) kind = EXIT_TRANS;
-                else kind = (ph.flags & F_FETAL) ? EXIT_SURF_FETAL : EXIT_SURF;
-                ph.exit_w = ph.w * P.exitScale;
-                ph.flags = (ph.flags & ~(3u << EXIT_SHIFT)) | (kind << EXIT_SHIFT);
-                ph.w = 0.0f;
-            }
-            const int prev = ph.curr;
-            ph.curr = newID;
-            ph.refTri = tri;
-            if (newID == P.fetal_id) ph.flags |= F_FETAL;
-            ph.unfin = Exact ? (step - thit) * m.mut : fmaxf(step - thit, 0.0f) * m.mut;
-            if (newID != prev) {
-                if (ph.region_acc) atomicAdd(s_region + prev, ph.region_acc);
-                ph.region_acc = 0;
-                if (Grad) {
-                    ga->L[prev] += ph.seg_len + thit;
-                    ga->k[prev] += ph.seg_k;
-                    ph.seg_len = 0.0f;
-                    ph.seg_k = 0;
-                }
-            } else if (Grad) {
-                ph.seg_len += thit;
-            }
-        } else {
-            ph.w = 0.0f;   // debug build: a triangle index out of range ends the photon
-        }
+        boundary_event<Exact, Grad>(P, s_media, s_region, s_cnt, ph, ga, tri, thit, step, pd.u1);
     } else {
         cnt.scatter++;
         ph.px = ph.px + step * ph.vx;
@@ -536,7 +599,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
             ph.absorbed = ph.w * m.alb;
             ph.w -= ph.absorbed;
         }
-        const V3 vn = scatter_direction<Exact>(v, m, rng.u1, rng.u2);
+        const V3 vn = scatter_direction<Exact>(v, m, pd.u1, pd.u2);
         ph.vx = vn.x; ph.vy = vn.y; ph.vz = vn.z;
         const V3 pr = v3(ph.px - P.poix, ph.py - P.poiy, ph.pz - P.poiz);
         const float cx = dot3(v3(P.nxx, P.nxy, P.nxz), pr);
@@ -609,7 +672,7 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
     }
     if (ph.w < P.w_th && ph.w > 0.0f) {
         cnt.roulette++;
-        if (rng.u3 < P.chance) {
+        if (pd.u3 < P.chance) {
             ph.w /= P.chance;
             ph.flags |= F_ROULETTE;
         } else {
@@ -623,6 +686,22 @@ __device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M,
         ph.w = 0.0f;
     }
     return ph.w > 0.0f && (ph.w > P.w_th || (ph.flags & F_ROULETTE));
+}
+
+// One iteration of the reference's do-while loop, the three parts in turn.  Returns false
+// when the photon ends.
+template <bool Exact, bool Grad, int STACK = kStackDepth, bool Agg = false>
+__device__ __forceinline__ bool step_photon(const KParams &P, const MeshView &M, const Medium *s_media,
+                                            unsigned long long *s_region, unsigned long long *s_cnt,
+                                            Photon &ph, Counters &cnt, GradAcc *ga)
+{
+    Pending pd;
+    const int st = propose_step<Exact>(P, s_media, ph, cnt, pd);
+    if (st == kStepEnded) return false;
+    float thit = kNoHit;
+    int tri = -1;
+    if (st == kStepQuery) tri = query_step<STACK>(P, M, s_media, ph, cnt, pd, thit);
+    return complete_step<Exact, Grad, Agg>(P, s_media, s_region, s_cnt, ph, cnt, ga, pd, tri, thit);
 }
 
 struct SmemLayout {

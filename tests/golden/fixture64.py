@@ -34,7 +34,7 @@ SPEC = {
     "plain_slab": dict(workload=("plain_slab", {}), n=500_000, B=20, seed=0x64_0011,
                        blocks={"sft": (1, 1, 1), "rtd": (1, 1, 1), "rz": (1, 1, 1), "vox": (3, 5, 5),
                                "vox_l2": (1, 1, 1)}),
-    "abdomen660": dict(workload=("curved_abdomen", {"wavelength": 660, "freq": 12}), n=200_000, B=20,
+    "abdomen660": dict(workload=("curved_abdomen", {"wavelength": 660, "freq": 12}), n=200_000, B=40,
                        seed=0x64_0660,
                        blocks={"sft": (4, 4, 1), "rtd": (2, 4, 1), "rz": (4, 4, 1), "vox": (10, 10, 10),
                                "vox_l2": (5, 5, 5)}),
