@@ -227,12 +227,6 @@ int lp_set_cell_lists(lp_ctx *ctx, int enable);
  * distance bounds from the planes of the listed triangles, at the cost of longer lists.
  * Results do not depend on it.  No reference counterpart. */
 int lp_set_cell_margin(lp_ctx *ctx, float cells);
-/* Query path of the transport kernel (no reference counterpart; results do not depend
- * on it): bit 0 carries each photon's lower bound of its distance to the mesh from step
- * to step, bit 1 reads the cell word ahead of the random numbers on every step, bit 2
- * answers a short step from its own cell's widened list (lp_set_cell_margin) with a
- * bound from the listed triangles' planes.  Default 7. */
-int lp_set_query_path(lp_ctx *ctx, uint32_t flags);
 /* Warp-aggregated absorption tallies (no reference counterpart; the reference's r-z
  * tally is a racy read-modify-write, MCLightPropagation.cl:254-271): enable = 1 makes
  * the lanes of a warp that deposit into the same r-z cell or voxel in the same step sum

@@ -113,7 +113,6 @@ _SIGS = {
     "lp_set_cell_lists": ([C.c_void_p, C.c_int], C.c_int),
     "lp_set_cell_margin": ([C.c_void_p, C.c_float], C.c_int),
     "lp_set_tally_aggregation": ([C.c_void_p, C.c_int], C.c_int),
-    "lp_set_query_path": ([C.c_void_p, C.c_uint32], C.c_int),
     "lp_set_smem_budget": ([C.c_void_p, C.c_int32], C.c_int),
     "lp_set_exit_records": ([C.c_void_p, C.c_int64], C.c_int),
     "lp_run": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),

@@ -252,7 +252,6 @@ struct lp_ctx {
     // lists hold the triangles touching each cell widened by cell_margin cells on every side
     float cell_margin = 0.5f;
     bool agg_tallies = false;   // lp_set_tally_aggregation
-    uint32_t query_path = 7u;   // lp_set_query_path (kQueryCarry | kQueryPrefetch | kQueryOneList)
     int32_t g_n[3] = {0, 0, 0};
     float grid_ms = 0;
     // differentiation (lp_set_gradient / lp_forward / lp_backward)
@@ -560,7 +559,6 @@ void fill_params(lp_ctx *c, KParams &P, int64_t first, int64_t n, int nodes_smem
     P.boundary_push = c->exact ? 0.0f : c->g_push;
     P.tri_eps = c->exact ? 0.0f : 2e-6f;
     P.agg_tallies = c->agg_tallies ? 1 : 0;
-    P.query_path = c->query_path;
 }
 
 // Cell grid over the mesh bounds padded by one cell: cubic cells of size h chosen so
@@ -914,14 +912,6 @@ int lp_set_arithmetic(lp_ctx *c, int exact)
 {
     if (!c) return fail(nullptr, LP_ERR_INVALID, "lp_set_arithmetic: ctx is NULL");
     c->exact = exact != 0;
-    return LP_OK;
-}
-
-int lp_set_query_path(lp_ctx *c, uint32_t flags)
-{
-    if (!c) return LP_ERR_INVALID;
-    if (flags > 7u) return fail(c, LP_ERR_INVALID, "lp_set_query_path: flags %u", flags);
-    c->query_path = flags;
     return LP_OK;
 }
 

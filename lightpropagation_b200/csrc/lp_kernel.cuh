@@ -92,8 +92,6 @@ struct KParams {
     float boundary_push, tri_eps;
     // 1: absorption deposits are summed per cell across the warp before the atomic adds
     int32_t agg_tallies;
-    // query path switches (kQuery*), none of which changes a result
-    uint32_t query_path;
     // scratch: photon work counter
     unsigned long long *work;
 };
@@ -124,20 +122,6 @@ __device__ __forceinline__ bool in_range_dbg(unsigned long long *dbg, long long 
 #define LP_IN_RANGE(dbg, i, n) true
 #endif
 
-// Query path switches (KParams::query_path):
-//   kQueryCarry     carry the distance bound from step to step (less the steps taken);
-//                   without it every step starts from its cell's bound alone
-//   kQueryPrefetch  read the cell word before the Philox rounds on every step; without it
-//                   only when the carried bound is used up
-//   kQueryOneList   answer a short step from its own cell's (widened) list, with a bound
-//                   from the listed triangles' planes; without it from the lists of all
-//                   cells the step's box overlaps
-constexpr uint32_t kQueryCarry = 1u, kQueryPrefetch = 2u, kQueryOneList = 4u;
-#ifdef LP_QUERY_PATH_FIXED
-#define LP_QPATH(P) (LP_QUERY_PATH_FIXED)
-#else
-#define LP_QPATH(P) ((P).query_path)
-#endif
 
 constexpr uint32_t kCellEmpty = 0x80000000u;
 constexpr uint32_t kCellDense = 127u;
@@ -471,8 +455,10 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
 // an unlisted triangle lies at least g_margin + dface from p (dface: distance from p to
 // the cell's faces), and no segment from p of length <= reach = g_margin + dface - g_eps
 // can reach one.  For listed triangles the bound is their plane distance.  On a
-// triangle (ref_tri >= 0) the bound is 0.  Returns false, with safe still valid, when
-// bound > reach: the list alone does not decide the query then.
+// triangle (ref_tri >= 0) the bound is 0.  safe comes in holding a lower bound already
+// known (the photon's carried one) and leaves holding the larger of the two.  Returns
+// false, with safe still valid, when bound > reach: the list alone does not decide the
+// query then.
 __device__ __forceinline__ bool list_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
                                            uint32_t word, float &t_out, int &tri_out, float &safe)
 {
@@ -486,7 +472,7 @@ __device__ __forceinline__ bool list_query(const KParams &P, const MeshView &M, 
     }
     int bid = 0x7fffffff;
     for (uint32_t k = 0; k < cnt; ++k) test_tri_safe(M, __ldg(r + k), p, v, ref_tri, best, bid, s);
-    safe = ref_tri >= 0 ? 0.0f : fmaxf(s - P.g_eps, 0.0f);
+    safe = fmaxf(safe, ref_tri >= 0 ? 0.0f : fmaxf(s - P.g_eps, 0.0f));
     if (!(bound <= reach)) return false;
     if (bid == 0x7fffffff) {
         t_out = kNoHit;

@@ -476,11 +476,10 @@ template <bool Exact>
 __device__ __forceinline__ int propose_step(const KParams &P, const Medium *s_media, Photon &ph, Counters &cnt,
                                             Pending &pd)
 {
-    // With no distance bound left (after a boundary, or once the steps have used it up)
-    // the step surely needs the cell word: its load is issued before the Philox rounds so
-    // that they hide its latency.  Otherwise it is read only if the step exceeds the bound.
-    const bool fresh = !(ph.safe > 0.0f) || (LP_QPATH(P) & kQueryPrefetch);
-    uint32_t word = fresh ? cell_at(P, ph.px, ph.py, ph.pz) : 0u;
+    // The cell word is read on every step, its load issued before the Philox rounds so
+    // that they hide its latency (reading it only when the carried bound is used up saves
+    // loads but waits on them: 1.3 % slower on the 660 nm abdomen).
+    const uint32_t word = cell_at(P, ph.px, ph.py, ph.pz);
     EventRng rng;
     rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
     [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
@@ -520,11 +519,10 @@ __device__ __forceinline__ int propose_step(const KParams &P, const Medium *s_me
         cnt.skip++;
         return kStepClear;
     }
-    if (!fresh) word = cell_at(P, ph.px, ph.py, ph.pz);
-    pd.word = word;
     if (word & kCellEmpty) {
-        // a cell no triangle touches: its word holds a bound for all its points
-        pd.safe_here = safe_distance(P, word);
+        // a cell no triangle touches: its word holds a bound for all its points (the
+        // larger of two lower bounds is one too)
+        pd.safe_here = fmaxf(pd.safe_here, safe_distance(P, word));
         if (reach < pd.safe_here) {
             cnt.skip++;
             return kStepClear;
@@ -549,15 +547,13 @@ __device__ __forceinline__ int query_step(const KParams &P, const MeshView &M, c
     }
     const uint32_t word = pd.word;
     bool done = false;
-    if (word & kCellEmpty) {
-        // pd.safe_here holds the empty cell's bound, which the step exceeds
-    } else if ((LP_QPATH(P) & kQueryOneList) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
+    // an empty cell: pd.safe_here holds its bound, which the step exceeds; a dense cell,
+    // or a grid without lists: the carried bound stays
+    if (!(word & kCellEmpty) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
         // the cell's own list: a bound from the planes of its triangles, and the
         // query itself when the step stays inside the widened cell
         done = list_query(P, M, p, v, ph.refTri, pd.reach, word, thit, tri, pd.safe_here);
         if (done) cnt.query++;
-    } else {
-        pd.safe_here = 0.0f;
     }
     if (!done) {
         bool used_bvh;
@@ -590,7 +586,7 @@ __device__ __forceinline__ bool complete_step(const KParams &P, const Medium *s_
         ph.py = ph.py + step * ph.vy;
         ph.pz = ph.pz + step * ph.vz;
         ph.refTri = -1;
-        ph.safe = (LP_QPATH(P) & kQueryCarry) ? fmaxf(safe_here - step - P.step_eps, 0.0f) : 0.0f;
+        ph.safe = fmaxf(safe_here - step - P.step_eps, 0.0f);
         if (Grad) {
             ph.seg_len += step;
             ph.seg_k++;

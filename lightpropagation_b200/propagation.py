@@ -189,11 +189,6 @@ class Simulation:
         touching its cell widened by this much (results are unchanged)."""
         self._ck(self._L.lp_set_cell_margin(self._h, float(cells)))
 
-    def set_query_path(self, flags: int):
-        """Query path switches (bit 0 carry the distance bound, bit 1 read the cell word
-        every step, bit 2 one-list queries); results are unchanged."""
-        self._ck(self._L.lp_set_query_path(self._h, int(flags)))
-
     def set_tally_aggregation(self, enable: bool):
         """Sum same-cell absorption deposits across the warp before the atomic adds
         (tallies are identical either way)."""
