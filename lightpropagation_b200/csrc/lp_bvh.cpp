@@ -284,7 +284,7 @@ int32_t build_par(Prim *pr, std::vector<BNode> &nodes, int64_t first, int64_t co
 
 }  // namespace
 
-void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
+void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target, int threads)
 {
     out = Bvh();
     std::vector<Prim> pr((size_t)n);
@@ -314,7 +314,7 @@ void build_bvh(const float *tri, int64_t n, Bvh &out, int leaf_target)
     std::vector<BNode> nodes;
     nodes.reserve((size_t)(2 * n / std::max(1, leaf_target) + 4));
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int n_threads = (int)std::min(hw, 16u);
+    const int n_threads = threads > 0 ? std::min(threads, 64) : (int)std::min(hw, 16u);
     if (n < 32768 || n_threads == 1) {
         build_par(pr.data(), nodes, 0, n, leaf_target, 0, 1);
     } else {

@@ -39,7 +39,9 @@ struct Bvh {
 
 constexpr int kLeafMax = 8;
 
-// Builds the tree over n_tri triangles given as 9 floats (K, L, M) each.
-void build_bvh(const float *tri, int64_t n_tri, Bvh &out, int leaf_target = 4);
+// Builds the tree over n_tri triangles given as 9 floats (K, L, M) each.  threads: the
+// worker threads of a large build (0: the hardware's, at most 16); the tree is the same
+// for every thread count.
+void build_bvh(const float *tri, int64_t n_tri, Bvh &out, int leaf_target = 4, int threads = 0);
 
 }  // namespace lp

@@ -7,7 +7,9 @@ both sides of that size and for a mesh of coincident triangles:
     reference's (M, E = K - M, F = L - M) of FindTriangleInPath (.cl:1037-1093);
   * every child box contains all vertices of the triangles below it;
   * the depth fits the device traversal stack (64);
-  * two builds of the same mesh give the same bytes.
+  * two builds of the same mesh give the same bytes;
+  * the tree does not depend on the number of worker threads (1, 2, 8, 16 threads give
+    the same bytes, whatever the test machine's own core count).
 """
 import os
 import subprocess
@@ -34,10 +36,10 @@ def dump_exe(tmp_path_factory):
     return str(out)
 
 
-def build(exe, tri, tmp_path, tag):
+def build(exe, tri, tmp_path, tag, threads=0):
     src, dst = tmp_path / f"{tag}.f32", tmp_path / f"{tag}.bin"
     np.ascontiguousarray(tri, np.float32).tofile(src)
-    subprocess.check_call([exe, str(src), str(dst)])
+    subprocess.check_call([exe, str(src), str(dst)] + ([str(threads)] if threads else []))
     raw = dst.read_bytes()
     nn, nt, depth = np.frombuffer(raw[:12], np.int32)
     margin = np.frombuffer(raw[12:16], np.float32)[0]
@@ -104,3 +106,19 @@ def test_bvh_tree_is_valid_and_deterministic(dump_exe, tmp_path, case):
     raw2, _, _, _ = build(dump_exe, tri, tmp_path, "b")
     assert raw1 == raw2, "two builds of the same mesh differ"
     check_tree(tri, depth, margin, arrs)
+
+
+@pytest.mark.parametrize("case", ["abdomen_52900", "coincident_40000"])
+def test_bvh_tree_does_not_depend_on_the_thread_count(dump_exe, tmp_path, case):
+    """One worker thread runs the serial build (build_from); 2, 8 and 16 run the parallel
+    recursion (build_par) and the threaded binning of large nodes.  All give the same tree."""
+    if case == "abdomen_52900":
+        tri, _, _ = meshes.curved_abdomen(freq=23)
+    else:
+        one = np.array([0, 0, 0, 1, 0, 0, 0, 1, 0], np.float32)
+        tri = np.tile(one, (40000, 1))
+    tri = np.asarray(tri, np.float32).reshape(-1, 9)
+    ref, _, _, _ = build(dump_exe, tri, tmp_path, "t1", threads=1)
+    for k in (2, 8, 16):
+        raw, _, _, _ = build(dump_exe, tri, tmp_path, f"t{k}", threads=k)
+        assert raw == ref, f"the tree built on {k} threads differs from the one-thread tree"
