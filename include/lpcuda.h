@@ -196,6 +196,14 @@ const char *lp_batch_last_error(const lp_batch *b);
 int lp_batch_set_instances(lp_batch *b, int32_t n_inst, const lp_instance *inst);
 /* Differentiation for every instance (see lp_set_gradient). */
 int lp_batch_set_gradient(lp_batch *b, int enable);
+/* Instances of at least `photons` photons run as a persistent transport launch of their
+ * own inside the batch's graph (the rest share the batch launch); photons <= 0: all
+ * share it.  Default 2^20: the batch kernel's instance switching costs every photon a
+ * little, a launch of its own costs one drain, and the two meet near 7e5 photons on the
+ * abdomen.  Tallies are the same either way. */
+int lp_batch_set_plain_threshold(lp_batch *b, int64_t photons);
+/* Instances the current setting runs as launches of their own. */
+int lp_batch_plain_count(const lp_batch *b, int32_t *count);
 /* Launch configuration: -1 (default) autotunes on the first run; 0..count-1 fixes one. */
 int lp_batch_config_count(void);
 int lp_batch_config_info(int32_t config, int32_t *block, int32_t *min_blocks, int32_t *stack);
@@ -242,8 +250,8 @@ int lp_set_exit_records(lp_ctx *ctx, int64_t capacity);
 
 /* --- run -------------------------------------------------------------------- */
 /* CalculatePropagation::Init + Propagation -> ExecKernel (CP.cpp:2003-2025, 1389-1759):
- * traces photons [first, first + n) in one persistent launch and adds their tallies.
- * Blocks until done. */
+ * traces photons [first, first + n) in one persistent launch (several in order when n
+ * exceeds 2^31, with the same tallies) and adds their tallies.  Blocks until done. */
 int lp_run(lp_ctx *ctx, int64_t first, int64_t n);
 /* As lp_run but returns after the launch is queued on the context's stream. */
 int lp_run_async(lp_ctx *ctx, int64_t first, int64_t n);
@@ -327,6 +335,7 @@ int lp_debug_fail_allocation(int64_t after);
  *   - dimensions must be finite and positive, and every image extent (dimensions /
  *     det_grid, 90 / det_grid[5]) below 2^20 cells, else LP_ERR_INVALID / LP_ERR_RANGE;
  *   - photons stop after LP_NOALLOC_MAX_STEPS steps (counted in LP_C_CAPPED);
+ *   - n_photons is at most 2^31 per call (LP_ERR_RANGE beyond; an lp_instance likewise);
  *   - nmuasg is a HOST pointer (n, mua, mus, g per region), copied into kernel params;
  *   - sft, rtd, rz, region are DEVICE outputs in the lp_tallies layouts (sizes as
  *     lp_get_geometry reports for the same dimensions and grid); results are ADDED to

@@ -141,6 +141,8 @@ _SIGS = {
     "lp_batch_last_error": ([C.c_void_p], C.c_char_p),
     "lp_batch_set_instances": ([C.c_void_p, C.c_int32, C.POINTER(Instance)], C.c_int),
     "lp_batch_set_gradient": ([C.c_void_p, C.c_int], C.c_int),
+    "lp_batch_set_plain_threshold": ([C.c_void_p, C.c_int64], C.c_int),
+    "lp_batch_plain_count": ([C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "lp_batch_set_config": ([C.c_void_p, C.c_int32], C.c_int),
     "lp_batch_autotune": ([C.c_void_p, C.c_int64, _ip, _dp], C.c_int),
     "lp_batch_run": ([C.c_void_p], C.c_int),

@@ -86,6 +86,17 @@ class Batch:
     def set_gradient(self, enable: bool):
         self._ck(self._L.lp_batch_set_gradient(self._h, 1 if enable else 0))
 
+    def set_plain_threshold(self, photons: int):
+        """Instances of at least `photons` photons run as a transport launch of their own
+        inside the batch's graph (<= 0: all share the batch launch; default 2^20)."""
+        self._ck(self._L.lp_batch_set_plain_threshold(self._h, int(photons)))
+
+    def plain_count(self) -> int:
+        """Instances the current setting runs as launches of their own."""
+        n = C.c_int32()
+        self._ck(self._L.lp_batch_plain_count(self._h, C.byref(n)))
+        return n.value
+
     def set_config(self, config: int):
         self._ck(self._L.lp_batch_set_config(self._h, int(config)))
 

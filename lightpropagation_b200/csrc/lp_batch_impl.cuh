@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const __grid_constan
             exhausted = base + 32ull >= n;
             const unsigned long long idx = base + lane;
             if (idx < n) {
-                start_photon(S.P, ph, S.P.first + (int64_t)idx);
+                start_photon(S.P, ph, (uint32_t)idx);
                 if (Grad) zero_grad(ga, S.P.n_media);
                 alive = true;
             }
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const __grid_constan
             if (!alive) {
                 const unsigned long long idx = base + __popc(need & lt_mask);
                 if (idx < n) {
-                    start_photon(S.P, ph, S.P.first + (int64_t)idx);
+                    start_photon(S.P, ph, (uint32_t)idx);
                     if (Grad) zero_grad(ga, S.P.n_media);
                     alive = true;
                 }

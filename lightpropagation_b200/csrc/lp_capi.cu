@@ -1064,19 +1064,29 @@ int lp_run_async(lp_ctx *c, int64_t first, int64_t n)
         LP_CUDA(c, c->exact ? lp::transport_occupancy_exact(smem, &per_sm)
                             : lp::transport_occupancy_fast(smem, &per_sm));
     if (per_sm < 1) return fail(c, LP_ERR_CUDA, "lp_run: transport kernel does not fit on an SM");
-    KParams P;
-    fill_params(c, P, first, n, nodes_smem, tris_smem);
-    LP_CUDA(c, cudaMemsetAsync(c->work.p, 0, 8, c->stream));
     if (c->exit_cap > 0) LP_CUDA(c, cudaMemsetAsync(c->exit_rec.p, 0, (size_t)c->exit_cap * 32, c->stream));
     LP_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    c->h2d_bytes += (int64_t)sizeof(KParams);
     c->st_nodes_smem = nodes_smem;
     c->st_tris_smem = tris_smem;
     c->st_smem = smem;
     c->st_per_sm = per_sm;
     c->st_grid = c->num_sms * per_sm;
-    LP_CUDA(c, c->exact ? lp::launch_transport_exact(P, c->num_sms * per_sm, smem, c->stream)
-                        : lp::launch_transport_fast(P, c->num_sms * per_sm, smem, c->stream));
+    // The kernel indexes the photons of one launch with 32 bits: a longer range runs as
+    // several launches in order (the same photon ids, so the same tallies).  Exit records
+    // (at most 2^30 slots, indexed from the range's first photon) all come from the first.
+    for (int64_t off = 0; off < n; off += lp::kMaxLaunchPhotons) {
+        const int64_t m = std::min<int64_t>(n - off, lp::kMaxLaunchPhotons);
+        KParams P;
+        fill_params(c, P, first + off, m, nodes_smem, tris_smem);
+        if (off > 0) {
+            P.exit_rec = nullptr;
+            P.exit_cap = 0;
+        }
+        LP_CUDA(c, cudaMemsetAsync(c->work.p, 0, 8, c->stream));
+        c->h2d_bytes += (int64_t)sizeof(KParams);
+        LP_CUDA(c, c->exact ? lp::launch_transport_exact(P, c->num_sms * per_sm, smem, c->stream)
+                            : lp::launch_transport_fast(P, c->num_sms * per_sm, smem, c->stream));
+    }
     LP_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     c->launched = true;
     return LP_OK;
@@ -1404,6 +1414,18 @@ struct lp_batch {
     int grid = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // Instances of at least plain_min photons (plain_min > 0) run as a persistent transport
+    // launch of their own inside the graph, with their context's shared-memory plan; the
+    // batch kernel sees them with no photons.  The batch kernel pays for its per-warp
+    // instance switching on every photon, a launch of its own only once (its drain):
+    // at about 7e5 photons the two cost the same on the abdomen.
+    struct PlainLaunch {
+        KParams P;
+        int grid = 0, smem = 0;
+    };
+    int64_t plain_min = int64_t(1) << 20;
+    std::vector<PlainLaunch> plain;
+    DevBuf<unsigned long long> plain_work;
     float last_ms = 0.0f;
     std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det, h_cnt;
     std::vector<double> h_grad;
@@ -1447,6 +1469,7 @@ int upload_instances(lp_batch *b)
     const size_t I = b->inst.size();
     std::vector<KParams> P(I);
     std::vector<Medium> M(I * lp::kBatchMedia);
+    b->plain.clear();
     for (size_t i = 0; i < I; ++i) {
         const lp_instance &in = b->inst[i];
         lp_ctx *c = b->ctx[in.context];
@@ -1474,6 +1497,21 @@ int upload_instances(lp_batch *b)
         p.exit_rec = nullptr;
         p.exit_cap = 0;
         p.work = nullptr;
+        if (b->plain_min > 0 && in.n_photons >= b->plain_min) {
+            lp_batch::PlainLaunch L;
+            L.P = p;
+            int ns = 0, ts = 0;
+            smem_plan(c, c->smem_budget, ns, ts);
+            L.P.nodes_smem = ns;
+            L.P.tris_smem = ts;
+            L.smem = lp::smem_bytes(ns, ts);
+            b->plain.push_back(L);
+            p.n = 0;
+        }
+    }
+    if (!b->plain.empty()) {
+        LP_BCUDA(b, b->plain_work.ensure(b->plain.size()));
+        for (size_t k = 0; k < b->plain.size(); ++k) b->plain[k].P.work = b->plain_work.p + k;
     }
     if (I) {
         LP_BCUDA(b, cudaMemcpyAsync(b->params.p, P.data(), I * sizeof(KParams), cudaMemcpyHostToDevice, b->stream));
@@ -1500,6 +1538,29 @@ int enqueue_zero(lp_batch *b)
     LP_BCUDA(b, cudaMemsetAsync(b->grad.p, 0, I * grad_stride(b) * 8, s));
     LP_BCUDA(b, cudaMemsetAsync(b->claimed.p, 0, I * 8, s));
     LP_BCUDA(b, cudaMemsetAsync(b->frontier.p, 0, 4, s));
+    if (!b->plain.empty()) LP_BCUDA(b, cudaMemsetAsync(b->plain_work.p, 0, b->plain.size() * 8, s));
+    return LP_OK;
+}
+
+// Grids of the plain launches: SMs x resident blocks of the transport kernel with each
+// launch's shared memory (queried outside stream capture).
+int prepare_plain(lp_batch *b)
+{
+    std::lock_guard<std::mutex> launch_lock(lp::launch_mutex());
+    for (lp_batch::PlainLaunch &L : b->plain) {
+        int per_sm = 0;
+        LP_BCUDA(b, b->grad_on ? lp::transport_occupancy_fast_grad(L.smem, &per_sm)
+                               : lp::transport_occupancy_fast(L.smem, &per_sm));
+        if (per_sm < 1) return bfail(b, LP_ERR_CUDA, "batch: transport kernel does not fit on an SM");
+        L.grid = b->num_sms * per_sm;
+    }
+    return LP_OK;
+}
+
+int enqueue_plain(lp_batch *b)
+{
+    for (const lp_batch::PlainLaunch &L : b->plain)
+        LP_BCUDA(b, lp::launch_transport_fast(L.P, L.grid, L.smem, b->stream));
     return LP_OK;
 }
 
@@ -1659,6 +1720,8 @@ int lp_batch_set_instances(lp_batch *b, int32_t n_inst, const lp_instance *in)
                          b->ctx[x.context]->max_region);
         if (x.n_photons < 0 || x.first < 0)
             return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: negative photon range", i);
+        if (x.n_photons > lp::kMaxLaunchPhotons)
+            return bfail(b, LP_ERR_RANGE, "lp_batch_set_instances: instance %d: more than 2^31 photons", i);
         for (int k = 0; k < 4 * x.n_media; ++k)
             if (!std::isfinite(x.nmuasg[k]))
                 return bfail(b, LP_ERR_INVALID, "lp_batch_set_instances: instance %d: non-finite media", i);
@@ -1682,7 +1745,29 @@ int lp_batch_set_instances(lp_batch *b, int32_t n_inst, const lp_instance *in)
         LP_BCUDA(b, b->params.ensure(J));
     }
     b->inst.assign(in, in + n_inst);
+    // the plain launches hold their parameters by value in the graph
+    const bool had_plain = !b->plain.empty();
+    const int r = upload_instances(b);
+    if (had_plain || !b->plain.empty()) drop_graph(b);
+    return r;
+}
+
+int lp_batch_set_plain_threshold(lp_batch *b, int64_t photons)
+{
+    if (!b) return fail(nullptr, LP_ERR_INVALID, "lp_batch_set_plain_threshold: batch is NULL");
+    if (photons == b->plain_min) return LP_OK;
+    b->plain_min = photons;
+    drop_graph(b);
+    if (b->inst.empty()) return LP_OK;
+    LP_BCUDA(b, cudaSetDevice(b->device));
     return upload_instances(b);
+}
+
+int lp_batch_plain_count(const lp_batch *b, int32_t *count)
+{
+    if (!b || !count) return fail(nullptr, LP_ERR_INVALID, "lp_batch_plain_count: NULL argument");
+    *count = (int32_t)b->plain.size();
+    return LP_OK;
 }
 
 int lp_batch_set_gradient(lp_batch *b, int enable)
@@ -1761,10 +1846,13 @@ int lp_batch_run(lp_batch *b)
         if ((r = lp_batch_autotune(b, 4000000, &best, nullptr))) return r;
     }
     if (!b->exec) {
-        // one graph: zero every instance's tallies and counters, then the persistent launch
+        // one graph: zero every instance's tallies and counters, the plain launches of
+        // the large instances, then the persistent batch launch
         if ((r = prepare_grid(b, b->config))) return r;
+        if ((r = prepare_plain(b))) return r;
         LP_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         r = enqueue_zero(b);
+        if (!r) r = enqueue_plain(b);
         if (!r) r = enqueue_launch(b, b->config);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->stream, &g);

@@ -16,6 +16,8 @@ constexpr int kMaxDet = 32;
 constexpr int kStackDepth = 64;
 constexpr int kGradRegions = 8;      // regions a differentiated run may have
 constexpr float kNoHit = 10000.0f;   // FindTriangleInPath's initial distance (.cl:1042)
+// photons of one transport launch: the kernels index them with 32 bits
+constexpr int64_t kMaxLaunchPhotons = int64_t(1) << 31;
 
 struct Medium {
     float n, mua, mus, g;

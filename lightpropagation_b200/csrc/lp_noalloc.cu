@@ -245,6 +245,8 @@ extern "C" int lp_run_noalloc(const lp_noalloc_args *a, void *stream)
     if (a->n_media < 1 || a->n_media > LP_NOALLOC_MAX_MEDIA)
         return reject(LP_ERR_RANGE, "lp_run_noalloc: n_media must be 1..LP_NOALLOC_MAX_MEDIA (64)");
     if (a->n_photons < 0 || a->first < 0) return reject(LP_ERR_INVALID, "lp_run_noalloc: negative photon range");
+    if (a->n_photons > lp::kMaxLaunchPhotons)
+        return reject(LP_ERR_RANGE, "lp_run_noalloc: more than 2^31 photons in one call");
     if (!(a->chance > 0.0f && a->chance <= 1.0f) || !(a->factor > 0.0f) || !(a->w_threshold >= 0.0f))
         return reject(LP_ERR_INVALID, "lp_run_noalloc: bad chance, factor or weight threshold");
     for (int i = 0; i < 6; ++i)

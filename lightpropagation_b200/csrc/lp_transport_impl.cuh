@@ -44,13 +44,14 @@ constexpr int kBlock = 256;
 struct Photon {
     float px, py, pz, vx, vy, vz;
     float w, unfin, absorbed;
-    float nvx, nvy, nvz;     // last boundary normal (CalcAlphaOut, .cl:1583)
+    int32_t last_tri;        // face of the last boundary event, -1 before any: its normal is
+                             // CalcAlphaOut's (.cl:1583), see photon_normal
     float exit_w;            // exit weight once scored
     int32_t curr, refTri;
     uint32_t steps;
-    uint32_t flags;          // bit0 traversedFetalTissue, bit1 roulette, bits 2-3 exit kind
+    uint32_t flags;          // see F_*, EXIT_SHIFT, AXIS_SHIFT
     unsigned long long region_acc;
-    int64_t pid;
+    uint32_t idx;            // photon index within the launch: the photon id is P.first + idx
     float seg_len;           // differentiation: path length and interactions in the
     uint32_t seg_k;          // current region since the photon entered it
     float safe;              // lower bound of the distance from the position to any triangle
@@ -62,7 +63,9 @@ struct GradAcc {
     float L[kGradRegions];
     uint32_t k[kGradRegions];
 };
-enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2 };
+// flags: bit 0 traversedFetalTissue, bit 1 roulette, bits 2-3 exit kind, bits 4-5 the
+// on-axis normal override at the last boundary (0 none, 1 +eZ, 2 -eZ, 3 zero vector)
+enum : uint32_t { F_FETAL = 1u, F_ROULETTE = 2u, EXIT_SHIFT = 2, AXIS_SHIFT = 4 };
 enum : uint32_t { EXIT_NONE = 0, EXIT_SURF = 1, EXIT_SURF_FETAL = 2, EXIT_TRANS = 3 };
 
 struct Counters {
@@ -217,11 +220,26 @@ static __device__ __noinline__ void score_gradient(const KParams &P, const GradA
     }
 }
 
+// The normal of the photon's last boundary event as the transport used it: the face's unit
+// normal, the on-axis override (sign * eZ), or (0, 0, -1) before any event (PhotonClass
+// init, .cl:344-389).  Kept as the face index and two flag bits instead of three floats.
+__device__ __forceinline__ V3 photon_normal(const KParams &P, const Photon &ph)
+{
+    const uint32_t axis = (ph.flags >> AXIS_SHIFT) & 3u;
+    if (axis) {
+        const float sg = axis == 1u ? 1.0f : (axis == 2u ? -1.0f : 0.0f);
+        return scl3(sg, v3(P.nzx, P.nzy, P.nzz));
+    }
+    if (ph.last_tri < 0) return v3(0.0f, 0.0f, -1.0f);
+    const float4 at = __ldg(P.tri_attr + ph.last_tri);
+    return v3(at.x, at.y, at.z);
+}
+
 // Exit record binning of CalculatePropagation.cpp:1553-1626 plus radial bins and rings.
 template <bool Grad>
 static __device__ __noinline__ void finish_photon(const KParams &P, const Photon &ph, const GradAcc *ga)
 {
-    const V3 v = v3(ph.vx, ph.vy, ph.vz), nv = v3(ph.nvx, ph.nvy, ph.nvz);
+    const V3 v = v3(ph.vx, ph.vy, ph.vz), nv = photon_normal(P, ph);
     const float alpha = fabsf(acosf(dot3(v, nv)));
     const V3 d = v3(P.poix - ph.px, P.poiy - ph.py, P.poiz - ph.pz);
     const float radius = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
@@ -233,7 +251,7 @@ static __device__ __noinline__ void finish_photon(const KParams &P, const Photon
     const float s = (kind == EXIT_SURF || kind == EXIT_SURF_FETAL) ? ph.exit_w : 0.0f;
     const float f = (kind == EXIT_SURF_FETAL) ? ph.exit_w : 0.0f;
     const float t = (kind == EXIT_TRANS) ? ph.exit_w : 0.0f;
-    const int64_t slot = ph.pid - P.first;
+    const int64_t slot = (int64_t)ph.idx;
     if (P.exit_rec && slot >= 0 && slot < P.exit_cap) {
         float4 *r = reinterpret_cast<float4 *>(P.exit_rec + 8 * slot);
         r[0] = make_float4(cx, cy, cz, s);
@@ -277,8 +295,9 @@ static __device__ __noinline__ void finish_photon(const KParams &P, const Photon
     }
 }
 
-__device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64_t pid)
+__device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, uint32_t idx)
 {
+    const int64_t pid = P.first + (int64_t)idx;
     // PhotonClass::Init (.cl:344-389) with vStart[0] (.cl:429-467)
     ph.px = P.p0x; ph.py = P.p0y; ph.pz = P.p0z;
     ph.vx = P.v0x; ph.vy = P.v0y; ph.vz = P.v0z;
@@ -303,14 +322,14 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
     ph.w = P.w0;
     ph.unfin = 0.0f;
     ph.absorbed = 0.0f;
-    ph.nvx = 0.0f; ph.nvy = 0.0f; ph.nvz = -1.0f;
+    ph.last_tri = -1;
     ph.exit_w = 0.0f;
     ph.curr = 0;
     ph.refTri = -1;
     ph.steps = 0;
     ph.flags = F_ROULETTE;
     ph.region_acc = 0;
-    ph.pid = pid;
+    ph.idx = idx;
     ph.seg_len = 0.0f;
     ph.seg_k = 0;
     ph.safe = 0.0f;
@@ -320,12 +339,14 @@ __device__ __forceinline__ void start_photon(const KParams &P, Photon &ph, int64
 // thit to the face `tri` (-1: no face, it leaves the model), then is transmitted or
 // reflected with probability from the Fresnel equations (xi against R).  Out of line: it
 // runs about once per hundred steps, and keeping its code out of the step loop keeps the
-// loop's instructions in cache for the warps that scatter.
+// loop's instructions in cache for the warps that scatter.  The photon goes in and comes
+// back by value: a reference would take its address out of the step loop, and the
+// compiler would then keep the photon in local memory on every step.
 template <bool Exact, bool Grad>
-static __device__ __noinline__ void boundary_event(const KParams &P, const Medium *s_media,
-                                                       unsigned long long *s_region, unsigned long long *s_cnt,
-                                                       Photon &ph, GradAcc *ga, int tri, float thit, float step,
-                                                       float xi)
+static __device__ __forceinline__ Photon boundary_event(const KParams &P, const Medium *s_media,
+                                                     unsigned long long *s_region, unsigned long long *s_cnt,
+                                                     Photon ph, GradAcc *ga, int tri, float thit, float step,
+                                                     float xi)
 {
     [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
     const Medium m = s_media[ph.curr];
@@ -350,13 +371,16 @@ static __device__ __noinline__ void boundary_event(const KParams &P, const Mediu
         if (ph.curr != inner && ph.curr != outer) atomicAdd(s_cnt + 14, 1ull);
         if (!LP_IN_RANGE(dbg, nxt_id, P.n_media)) nxt_id = ph.curr;
         const Medium nx = s_media[nxt_id];
+        uint32_t axis = 0u;
         if (P.compat & 0x2u) {
             if (fabsf(sqrtf(ph.px * ph.px + ph.py * ph.py)) < 0.01f) {
                 const float sg = sign_cl(dot3(nv, v3(P.ezx, P.ezy, P.ezz)));
                 nv = scl3(sg, v3(P.nzx, P.nzy, P.nzz));
+                axis = sg > 0.0f ? 1u : (sg < 0.0f ? 2u : 3u);
             }
         }
-        ph.nvx = nv.x; ph.nvy = nv.y; ph.nvz = nv.z;
+        ph.last_tri = tri;
+        ph.flags = (ph.flags & ~(3u << AXIS_SHIFT)) | (axis << AXIS_SHIFT);
         // TransmitOrReflect (.cl:921-1018)
         const float cosIn = dot3(nv, v);
         const float absCosIn = fabsf(cosIn);
@@ -452,6 +476,7 @@ static __device__ __noinline__ void boundary_event(const KParams &P, const Mediu
     } else {
         ph.w = 0.0f;   // debug build: a triangle index out of range ends the photon
     }
+    return ph;
 }
 
 // A step in three parts: propose_step draws the event's random numbers and the step
@@ -481,7 +506,7 @@ __device__ __forceinline__ int propose_step(const KParams &P, const Medium *s_me
     // loads but waits on them: 1.3 % slower on the 660 nm abdomen).
     const uint32_t word = cell_at(P, ph.px, ph.py, ph.pz);
     EventRng rng;
-    rng.draw((uint64_t)ph.pid, ph.steps + 1u, P.stream, P.key0, P.key1);
+    rng.draw((uint64_t)(P.first + (int64_t)ph.idx), ph.steps + 1u, P.stream, P.key0, P.key1);
     [[maybe_unused]] unsigned long long *const dbg = P.counters ? P.counters + kBoundsCounter : nullptr;
     if (!LP_IN_RANGE(dbg, ph.curr, P.n_media)) {
         ph.w = 0.0f;
@@ -579,7 +604,7 @@ __device__ __forceinline__ bool complete_step(const KParams &P, const Medium *s_
     const bool boundary = (tri >= 0) ? (thit <= (m.ambient ? step : reach)) : (kNoHit <= step);
     if (boundary) {
         cnt.boundary++;
-        boundary_event<Exact, Grad>(P, s_media, s_region, s_cnt, ph, ga, tri, thit, step, pd.u1);
+        ph = boundary_event<Exact, Grad>(P, s_media, s_region, s_cnt, ph, Grad ? ga : nullptr, tri, thit, step, pd.u1);
     } else {
         cnt.scatter++;
         ph.px = ph.px + step * ph.vx;
@@ -786,7 +811,7 @@ __global__ void __launch_bounds__(kBlock, LP_TRANSPORT_MIN_BLOCKS) transport_ker
             if (!alive) {
                 const unsigned long long idx = base + __popc(need & lt_mask);
                 if (idx < (unsigned long long)P.n) {
-                    start_photon(P, ph, P.first + (int64_t)idx);
+                    start_photon(P, ph, (uint32_t)idx);
                     if (Grad) {
                         for (int r = 0; r < P.n_media; ++r) {
                             ga.L[r] = 0.0f;

@@ -1,7 +1,8 @@
 """Batched transport on the GPU: every instance of one persistent launch must equal,
 bit for bit, a single-instance lp_run on its context with its media and photon range
 (integer tallies and event counters), for every launch configuration the autotuner can
-pick, across CUDA-graph replays and instance updates.  Gradient sums are FP64 atomics
+pick, across CUDA-graph replays and instance updates, and with the large instances run
+as transport launches of their own inside the graph.  Gradient sums are FP64 atomics
 whose order differs between launches, so they are compared to 1e-9 relative."""
 import numpy as np
 import pytest
@@ -118,6 +119,42 @@ def test_batch_gradient_equals_single(meshes2):
             bg = b.gradient(i)
             for k in ("signal", "d_mua", "d_mus"):
                 assert np.allclose(bg[k], g[k], rtol=1e-9, atol=0), k
+    for s in sims:
+        s.close()
+
+
+def test_large_instances_as_own_launches_equal_single_runs(meshes2):
+    """With the plain threshold at 2000 photons the instances of 3000, 4500 and 2500
+    photons run as transport launches of their own inside the graph, the rest in the batch
+    launch: every instance still equals its single run, with and without differentiation,
+    across a graph replay and an update of the instances."""
+    sims = [_sim(w) for w in meshes2]
+    insts = _instances(meshes2)
+    with Batch(sims) as b:
+        b.set_instances(insts)
+        b.set_config(0)
+        b.set_plain_threshold(2000)
+        assert b.plain_count() == 3
+        b.run()
+        for i, x in enumerate(insts):
+            _same(b.tallies(i), _single(meshes2, x)[0], x.nmuasg.shape[0])
+        new = [Instance(x.context, x.nmuasg * np.float32([1, 1.05, 0.95, 1]), x.n_photons, x.first + 11)
+               for x in insts]
+        b.set_instances(new)
+        b.run()
+        b.run()
+        for i, x in enumerate(new):
+            _same(b.tallies(i), _single(meshes2, x)[0], x.nmuasg.shape[0])
+        b.set_gradient(True)
+        b.run()
+        for i, x in enumerate(new):
+            t, g = _single(meshes2, x, grad=True)
+            _same(b.tallies(i), t, x.nmuasg.shape[0])
+            bg = b.gradient(i)
+            for k in ("signal", "d_mua", "d_mus"):
+                assert np.allclose(bg[k], g[k], rtol=1e-9, atol=0), k
+        b.set_plain_threshold(0)
+        assert b.plain_count() == 0
     for s in sims:
         s.close()
 

@@ -11,7 +11,9 @@
   * the NCCL reduction of run_sharded on one rank: the device-alias path of the
     multi-GPU code, integer tallies and FP64 differentiation sums;
   * the bounds-checked build (liblpcuda_debug.so, in place of compute-sanitizer, which
-    this pool does not offer) counts no out-of-range index and changes no tally.
+    this pool does not offer) counts no out-of-range index and changes no tally;
+  * a photon range longer than 2^31 (the kernel indexes a launch's photons with 32 bits)
+    runs as several launches with the tallies of the same range run as separate calls.
 """
 import datetime
 import os
@@ -214,3 +216,27 @@ def test_bounds_checked_build_finds_nothing_and_changes_nothing():
         for k in ("sft", "region", "det", "vox_sum"):
             assert dbg[key][k] == rel[key][k], (key, k)
         assert dbg[key]["counters"]["scatter"] == rel[key]["counters"]["scatter"]
+
+
+def test_range_beyond_2_31_photons_runs_in_chunks():
+    """2^31 + 1000 slab photons that end at their first roulette (weight threshold 1,
+    survival chance 1e-6): one lp_run over the whole range (two launches inside) against
+    lp_run over [0, 2^31) and then over the remaining 1000 photons on the same tallies."""
+    w = workloads.plain_slab()
+    w.w_threshold = 1.0
+    w.chance = 1e-6
+    n0 = 2 ** 31
+    with Simulation(0) as s:
+        w.apply(s, seed=5)
+        s.zero()
+        s.run(n0 + 1000, 0)
+        one = s.tallies()
+        s.zero()
+        s.run(n0, 0)
+        s.run(1000, n0)
+        two = s.tallies()
+    assert one["counters"]["photons"] == n0 + 1000
+    for key in KEYS:
+        assert np.array_equal(one[key], two[key]), key
+    for k in ("scatter", "boundary", "roulette"):
+        assert one["counters"][k] == two["counters"][k], k

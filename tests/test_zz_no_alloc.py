@@ -120,6 +120,9 @@ def test_noalloc_rejects_bad_dimensions():
     a.dimensions[:] = [10.0, 10.0, 10.0]
     a.det_grid[:] = [1.0, 1.0, 1.0, 1.0, 1.0, 1e-6]
     assert L.lp_run_noalloc(C.byref(a), None) == 5
+    a.det_grid[:] = [1.0] * 6
+    a.n_photons = 2 ** 31 + 1                                     # one call indexes photons with 32 bits
+    assert L.lp_run_noalloc(C.byref(a), None) == 5
 
 
 def test_noalloc_refuses_out_of_range_region_ids():
