@@ -52,6 +52,8 @@ enum {
     LP_C_BAD_INPUT,   /* lp_run_noalloc: triangles whose region ids failed the device-side check */
     LP_C_BOUNDS,      /* bounds-checked build (liblpcuda_debug.so): accesses skipped as out of range */
     LP_C_REGION_MISMATCH, /* boundary events whose face does not border the photon's region */
+    LP_C_AGG_LEADERS, /* aggregated tallies (lp_set_tally_aggregation): r-z deposit groups, one
+                         atomic each; 1 - groups / deposits is the warp match rate */
     LP_NCOUNTERS = 16
 };
 

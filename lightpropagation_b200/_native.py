@@ -18,7 +18,7 @@ COMPAT_EXIT_RSP, COMPAT_AXIS_NORMAL, COMPAT_SIGNED_FRESNEL, COMPAT_ALL = 1, 2, 4
 NCOUNTERS = 16
 COUNTER_NAMES = ["scatter", "boundary", "query", "roulette", "miss", "capped", "rz_drop",
                  "vox_drop", "photons", "draws", "safe_skip", "bvh_query", "bad_input", "bounds",
-                 "region_mismatch"]
+                 "region_mismatch", "agg_leaders"]
 FIX_ONE = float(2 ** 32)
 
 _fp = C.POINTER(C.c_float)

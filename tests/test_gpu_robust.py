@@ -240,3 +240,27 @@ def test_range_beyond_2_31_photons_runs_in_chunks():
         assert np.array_equal(one[key], two[key]), key
     for k in ("scatter", "boundary", "roulette"):
         assert one["counters"][k] == two["counters"][k], k
+
+
+@pytest.mark.parametrize("wname", ["slab", "abdomen"])
+def test_tally_aggregation_changes_nothing(wname):
+    """Warp-aggregated deposits (lanes that hit the same r-z cell or voxel are matched with
+    __match_any_sync, their fixed-point values summed, one atomic per group) give the plain
+    kernel's tallies bit for bit; the leader counter gives the match rate."""
+    w = workloads.plain_slab() if wname == "slab" else workloads.curved_abdomen(freq=12)
+    n = 200000
+    out = []
+    for agg in (False, True):
+        with Simulation(0) as s:
+            w.apply(s, seed=17)
+            s.set_tally_aggregation(agg)
+            s.zero()
+            s.run(n)
+            out.append(s.tallies())
+    for key in KEYS:
+        assert np.array_equal(out[0][key], out[1][key]), key
+    c = out[1]["counters"]
+    deposits = c["scatter"] - c["rz_drop"]
+    assert 0 < c["agg_leaders"] <= deposits
+    print(f"{wname}: r-z deposit groups {c['agg_leaders']} of {deposits} deposits, "
+          f"match rate {1 - c['agg_leaders'] / deposits:.3f}")

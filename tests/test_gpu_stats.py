@@ -118,6 +118,7 @@ def check_images(g, o, keys, dof):
         assert z.size > 10, (k, z.size)
         bound = t_bound(z.size, dof)
         report[k] = (z.size, float(np.abs(z).max()), float(np.mean(z * z)))
+        print(f"{k}: {z.size} bins, max |z| {report[k][1]:.2f} (bound {bound:.2f}), mean z^2 {report[k][2]:.3f}")
         assert np.abs(z).max() < bound, f"{k}: max |z| {np.abs(z).max():.2f} >= {bound:.2f} over {z.size} bins"
         # E[t^2] = dof / (dof - 2) for Student's t; allow for the correlation of bins
         assert np.mean(z * z) < 1.5 * dof / (dof - 2), f"{k}: mean z^2 {np.mean(z * z):.3f}"
@@ -148,6 +149,7 @@ def test_slab_scalar_tallies_vs_fp64_oracle(slab_pair):
     surface, fetal and transmitted weight and absorption per region, |z| < 3 each."""
     g, o, _ = slab_pair
     z = batch_z(g["scalars_b"], o["scalars_b"])
+    print("slab scalar z:", np.round(z, 2))
     assert np.all(np.abs(z) < 3), z
 
 
@@ -162,6 +164,7 @@ def test_slab_voxel_fluence_relative_l2(slab_pair):
     photons; the noise of the two runs explains most of what remains."""
     g, o, _ = slab_pair
     rel, noise = voxel_l2(g, o)
+    print(f"slab voxel relative L2 {rel:.4f}, noise of the two runs {noise:.4f}")
     assert rel < 0.01, (rel, noise)
     assert rel * rel - noise * noise < 0.005 ** 2, f"relative L2 {rel:.4f}, noise alone {noise:.4f}"
 
@@ -181,8 +184,9 @@ def test_abdomen_scalar_tallies_and_rings_vs_fp64_oracle(abdomen_pair):
     photons against 4e6 FP64-oracle photons, |z| < 3 per scalar tally and per ring."""
     g, o, _ = abdomen_pair
     z = batch_z(g["scalars_b"], o["scalars_b"])
-    assert np.all(np.abs(z) < 3), z
     zr = batch_z(g["det_b"][:, :, 0], o["det_b"][:, :, 0])
+    print(f"{o['name']} scalar z:", np.round(z, 2), "ring z:", np.round(zr, 2))
+    assert np.all(np.abs(z) < 3), z
     assert np.all(np.abs(zr) < 3), zr
 
 
@@ -195,6 +199,7 @@ def test_abdomen_images_vs_fp64_oracle(abdomen_pair):
 def test_abdomen_voxel_fluence_relative_l2(abdomen_pair):
     g, o, _ = abdomen_pair
     rel, noise = voxel_l2(g, o)
+    print(f"{o['name']} voxel relative L2 {rel:.4f}, noise of the two runs {noise:.4f}")
     assert rel < 0.01, (rel, noise)
 
 
@@ -207,6 +212,7 @@ def test_abdomen_derivatives_vs_fp64_perturbation_mc(abdomen_pair):
     za = batch_z(g["dmua_b"][:, :, 1:], oa[:, :, 1:])
     zs = batch_z(g["dmus_b"][:, :, 1:], os_[:, :, 1:])
     z = np.concatenate([za.ravel(), zs.ravel()])
+    print(f"{o['name']} derivatives: max |z| {np.abs(z).max():.2f} over {z.size}")
     assert z.size == 60
     bound = t_bound(z.size, min(g["B"], int(o["B"])) - 1, alpha=1e-2)
     assert np.abs(z).max() < bound, (np.abs(z).max(), bound)
