@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -1426,6 +1427,14 @@ struct lp_batch {
     int64_t plain_min = int64_t(1) << 20;
     std::vector<PlainLaunch> plain;
     DevBuf<unsigned long long> plain_work;
+    // The r-z and voxel tallies (the atomic targets of every scatter event) of the
+    // instances with a launch of their own sit in buffers of their own, like a context's:
+    // as slices of the batch's large arrays the same launch measured up to 15 % slower.
+    struct OwnTallies {
+        DevBuf<unsigned long long> rz, vox;
+    };
+    std::vector<std::unique_ptr<OwnTallies>> own;
+    std::vector<unsigned long long *> rz_of, vox_of;   // per instance: where its r-z, voxel tallies are
     float last_ms = 0.0f;
     std::vector<uint64_t> h_sft, h_rtd, h_rz, h_vox, h_rbins, h_region, h_det, h_cnt;
     std::vector<double> h_grad;
@@ -1470,6 +1479,8 @@ int upload_instances(lp_batch *b)
     std::vector<KParams> P(I);
     std::vector<Medium> M(I * lp::kBatchMedia);
     b->plain.clear();
+    b->rz_of.assign(I, nullptr);
+    b->vox_of.assign(I, nullptr);
     for (size_t i = 0; i < I; ++i) {
         const lp_instance &in = b->inst[i];
         lp_ctx *c = b->ctx[in.context];
@@ -1498,6 +1509,12 @@ int upload_instances(lp_batch *b)
         p.exit_cap = 0;
         p.work = nullptr;
         if (b->plain_min > 0 && in.n_photons >= b->plain_min) {
+            const size_t k = b->plain.size();
+            if (b->own.size() <= k) b->own.push_back(std::unique_ptr<lp_batch::OwnTallies>(new lp_batch::OwnTallies));
+            LP_BCUDA(b, b->own[k]->rz.ensure(std::max<size_t>(b->n_rz, 1)));
+            LP_BCUDA(b, b->own[k]->vox.ensure(std::max<size_t>(b->n_vox, 1)));
+            p.rz = b->own[k]->rz.p;
+            p.vox = b->own[k]->vox.p;
             lp_batch::PlainLaunch L;
             L.P = p;
             int ns = 0, ts = 0;
@@ -1508,7 +1525,10 @@ int upload_instances(lp_batch *b)
             b->plain.push_back(L);
             p.n = 0;
         }
+        b->rz_of[i] = p.rz;
+        b->vox_of[i] = p.vox;
     }
+    b->own.resize(b->plain.size());
     if (!b->plain.empty()) {
         LP_BCUDA(b, b->plain_work.ensure(b->plain.size()));
         for (size_t k = 0; k < b->plain.size(); ++k) b->plain[k].P.work = b->plain_work.p + k;
@@ -1539,6 +1559,10 @@ int enqueue_zero(lp_batch *b)
     LP_BCUDA(b, cudaMemsetAsync(b->claimed.p, 0, I * 8, s));
     LP_BCUDA(b, cudaMemsetAsync(b->frontier.p, 0, 4, s));
     if (!b->plain.empty()) LP_BCUDA(b, cudaMemsetAsync(b->plain_work.p, 0, b->plain.size() * 8, s));
+    for (size_t k = 0; k < b->plain.size(); ++k) {
+        LP_BCUDA(b, cudaMemsetAsync(b->own[k]->rz.p, 0, b->n_rz * 8, s));
+        if (b->n_vox) LP_BCUDA(b, cudaMemsetAsync(b->own[k]->vox.p, 0, b->n_vox * 8, s));
+    }
     return LP_OK;
 }
 
@@ -1917,9 +1941,9 @@ int lp_batch_get_tallies(lp_batch *b, int32_t i, lp_tallies *out)
     b->h_det.resize(DD * 2);
     LP_BCUDA(b, cudaMemcpyAsync(b->h_sft.data(), b->sft.p + i * b->n_sft, b->n_sft * 8, cudaMemcpyDeviceToHost, s));
     LP_BCUDA(b, cudaMemcpyAsync(b->h_rtd.data(), b->rtd.p + i * b->n_rtd, b->n_rtd * 8, cudaMemcpyDeviceToHost, s));
-    LP_BCUDA(b, cudaMemcpyAsync(b->h_rz.data(), b->rz.p + i * b->n_rz, b->n_rz * 8, cudaMemcpyDeviceToHost, s));
+    LP_BCUDA(b, cudaMemcpyAsync(b->h_rz.data(), b->rz_of[i], b->n_rz * 8, cudaMemcpyDeviceToHost, s));
     if (b->n_vox)
-        LP_BCUDA(b, cudaMemcpyAsync(b->h_vox.data(), b->vox.p + i * b->n_vox, b->n_vox * 8, cudaMemcpyDeviceToHost, s));
+        LP_BCUDA(b, cudaMemcpyAsync(b->h_vox.data(), b->vox_of[i], b->n_vox * 8, cudaMemcpyDeviceToHost, s));
     if (b->n_rbins)
         LP_BCUDA(b, cudaMemcpyAsync(b->h_rbins.data(), b->rbins.p + i * b->n_rbins, b->n_rbins * 8,
                                     cudaMemcpyDeviceToHost, s));
