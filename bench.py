@@ -28,7 +28,7 @@ roofline  FP32 issue bound: algorithmic FLOPs per photon
        photon, counted by the kernel) over the measured FP32 FMA peak of the device;
        beside it the L2-atomic fraction: absorption and exit deposits per second over
        the measured rate of 64-bit atomic adds to an L2-resident buffer.
-config1_slab  the like-for-like comparison: the 3-layer slab (config 1: pencil beam,
+config1_slab  the like-for-like comparison: the 3-layer slab (32 triangles, pencil beam,
        reference behaviours on, 1e6 photons) on the GPU and through the reference's
        own kernel source on the host cores, the same physics on both sides.
 cpu_baseline / --impl reference  the reference kernel source compiled for the CPU
@@ -403,7 +403,7 @@ def deposits_per_photon(c, n):
 
 
 def slab_section(args, local, peak):
-    """Config 1 on both sides with the same physics: the 3-layer slab, a pencil beam and
+    """The same physics on both sides: the 3-layer slab (32 triangles), a pencil beam and
     the reference behaviours on, 1e6 photons per launch.  GPU: device time of 5 launches
     and e2e through the public API; reference: its kernel source on all host cores."""
     from lightpropagation_b200 import Simulation, workloads

@@ -83,7 +83,7 @@ def test_gradient_sums_match_oracle(oracle_lib, case):
 
 
 def test_adjoint_matches_central_differences_all_120():
-    """All 120 derivatives of config 4 (5 tissue regions x 6 rings x (mua, mus) x 2
+    """All 120 derivatives of the ring signals (5 tissue regions x 6 rings x (mua, mus) x 2
     wavelengths, on the curved abdomen at 40,000 triangles): the adjoint sums of one
     differentiated pass against central differences (+-5 %, common random numbers: the
     same photon ids at both parameter values), B batches of n photons each

@@ -17,7 +17,7 @@ and the two are compared tally by tally:
     Carlo): |z| within the Bonferroni bound of Student's t.
 
 z = (mean_gpu - mean_oracle) / sqrt(se_gpu^2 + se_oracle^2), each se from its batches.
-GPU results are deterministic for a seed, so each test gives the same verdict every run.
+GPU results are deterministic for a seed, so each test gives the same outcome every run.
 """
 import os
 import sys
@@ -145,7 +145,7 @@ def slab_pair():
 
 
 def test_slab_scalar_tallies_vs_fp64_oracle(slab_pair):
-    """1e8 production photons on the plain slab (config 1) against 1e7 FP64-oracle photons:
+    """1e8 production photons on the 3-layer slab against 1e7 FP64-oracle photons:
     surface, fetal and transmitted weight and absorption per region, |z| < 3 each."""
     g, o, _ = slab_pair
     z = batch_z(g["scalars_b"], o["scalars_b"])
@@ -160,7 +160,7 @@ def test_slab_images_vs_fp64_oracle(slab_pair):
 
 
 def test_slab_voxel_fluence_relative_l2(slab_pair):
-    """The north-star bar: relative L2 of the 1 mm voxel absorption grid below 1% at 1e8
+    """The accuracy bar: relative L2 of the 1 mm voxel absorption grid below 1% at 1e8
     photons; the noise of the two runs explains most of what remains."""
     g, o, _ = slab_pair
     rel, noise = voxel_l2(g, o)
