@@ -3,14 +3,14 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-A step is one pass of the hot path over one batch: ``--photons`` photons (1e7 by
-default for the abdomen) traced through the mesh in one launch, tallies zeroed before
-and complete after.  The default workload is the curved-mesh abdomen (202,500
-triangles, fibre source, six ring detectors) at 660 nm and at 940 nm: steps alternate
-between the two optical-property tables on one mesh, so a job of K steps traces K/2
-batches at each wavelength; at K = 20 that is the workload's 1e8 photons per
-wavelength.  ``--photons 100000000`` runs 1e8 photons per launch.  ``--workload plain_slab``
-is the small 3-layer slab.  Photons are sharded by index range across ranks (weak
+A step is one pass of the hot path over one batch: ``--photons`` photons (1e8 by
+default for the abdomen, the workload's stated count per launch) traced through the
+mesh in one launch, tallies zeroed before and complete after.  The default workload is
+the curved-mesh abdomen (202,500 triangles, fibre source, six ring detectors) at 660 nm
+and at 940 nm: steps alternate between the two optical-property tables on one mesh, so
+a job of K steps traces about K/2 batches at each wavelength.  ``--photons 10000000``
+runs the shorter 1e7-photon launches.  ``--workload plain_slab`` is the small 3-layer
+slab.  Photons are sharded by index range across ranks (weak
 scaling: every rank traces the same number of photons per step); the integer
 tallies are summed over ranks with one NCCL all-reduce per launch, inside the
 timed region.
@@ -66,11 +66,11 @@ def env_int(k, d):
 def load_cases(name, photons):
     """The workloads the steps trace, in turn.  ``curved_abdomen`` (the default) is the
     curved-mesh abdomen at 660 nm and at 940 nm: one mesh, two optical-property tables,
-    1e7 photons per launch."""
+    1e8 photons per launch."""
     import dataclasses
     from lightpropagation_b200 import workloads
     if name == "curved_abdomen":
-        w = workloads.curved_abdomen(wavelength=660, n_photons=10_000_000)
+        w = workloads.curved_abdomen(wavelength=660, n_photons=100_000_000)
         nm940 = np.array(workloads.ABDOMEN_MEDIA[940], np.float32)
         cases = [w, dataclasses.replace(w, nmuasg=nm940, name=w.name.replace("660nm", "940nm"))]
     else:
@@ -692,7 +692,7 @@ def main():
     ap.add_argument("--workload", default="curved_abdomen",
                     help="curved_abdomen (660 + 940 nm per step), plain_slab, or another named workload")
     ap.add_argument("--photons", type=int, default=0,
-                    help="photons per launch per GPU (default: the workload's, 1e7 for the abdomen)")
+                    help="photons per launch per GPU (default: the workload's, 1e8 for the abdomen)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient-cost launches")
     ap.add_argument("--no-slab", action="store_true", help="skip the like-for-like config-1 slab section")
