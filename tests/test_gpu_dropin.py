@@ -12,6 +12,9 @@ make_golden.py), written back to reference-format files in a temporary directory
   * the Python launcher (lightpropagation_b200.CalculatePropagation) with the same
     setters and seed, whose images, written by the same log writers, must give the
     same files byte for byte;
+  * the log files lpsim wrote, parsed back: the surface array, the reflectance per
+    radius and the fluence per depth against the GPU images with the reference's scale
+    formulas (Logs.cpp:337-402, 521-561, 651-672, 1075-1110);
   * the images against the oracle with common random numbers: reference-order
     arithmetic on the GPU, the same Philox stream in the oracle (the FP32 restatement
     that is pinned to the reference kernel; the FP64 oracle for the curved model, where
@@ -159,3 +162,44 @@ def test_launcher_images_match_the_oracle_with_common_random_numbers(tmp_path, n
     # events per photon agree closely (the same trajectories, step for step)
     for k in ("scatter", "boundary"):
         assert abs(t["counters"][k] - r.counters[k]) <= 0.02 * r.counters[k], k
+
+
+def _read_log(path):
+    return np.array([[float(x) for x in line.split("\t") if x.strip()] for line in open(path) if line.strip()])
+
+
+@pytest.mark.parametrize("name", ["model1", "model4_curved"])
+def test_lpsim_logs_hold_the_gpu_images_in_the_reference_scales(tmp_path, name):
+    """The reference-format files lpsim writes from its GPU tallies, parsed back, against
+    the Python launcher's images of the same photons (same seed) with the reference's
+    formulas: SurfRxy.txt is the surface array (SaveSurfaceArr), SurfRxy_perRadius.txt
+    the reflectance summed over angles and scaled per ring area, 1 / ((ir + 1/2) 2 pi dr^2 N)
+    (ScalePerRadius1D), FluencePrz_perZ.txt the fluence summed over radii per depth row,
+    1 / (dz N) (FluenceZ).  The files hold 6 significant digits."""
+    n = PHOTONS[name]
+    _, cfg = write_model(name, str(tmp_path), n)
+    w = modelio.load_model(cfg)
+    out = tmp_path / "cpp"
+    out.mkdir()
+    r = subprocess.run([modelio.LPSIM, "-f", cfg, "-s", "-a", "-o", str(out), "--seed", str(SEED)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    cp = python_launcher(w, n, SEED, exact=False)
+    g = np.asarray(w.det_grid, np.float32)
+    dr, dz = float(g[3]), float(g[2])
+    sft = cp.GetSFTImage(0).data[:, :, 0]
+    assert np.allclose(_read_log(out / "SurfRxy.txt"), sft, rtol=1e-5, atol=0)
+    assert sft.sum() > 0
+    rtd = cp.GetRTdImage(0).data[:, :, 0]
+    pr = _read_log(out / "SurfRxy_perRadius.txt")
+    assert np.allclose(pr[:, 0], np.arange(rtd.shape[1]) * dr, rtol=1e-5)
+    s1 = np.float32(2.0 * np.pi * dr * dr * n)
+    want = [rtd[:, ir].sum(dtype=np.float32) * np.float32(1.0 / ((ir + 0.5) * float(s1))) for ir in range(rtd.shape[1])]
+    assert np.allclose(pr[:, 1], want, rtol=1e-4, atol=0)
+    img = cp.GetPhirzImage()
+    rz = img.data[:, :, 0]
+    pz = _read_log(out / "FluencePrz_perZ.txt")
+    assert np.allclose(pz[:, 0], [abs(img.extent[2] + j) * dz for j in range(rz.shape[0])], rtol=1e-5)
+    want = [rz[j, :].sum(dtype=np.float32) / np.float32(dz * n) for j in range(rz.shape[0])]
+    assert np.allclose(pz[:, 1], want, rtol=1e-4, atol=1e-30)
+    assert max(want) > 0
