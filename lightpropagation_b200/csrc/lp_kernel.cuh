@@ -486,4 +486,67 @@ __device__ __forceinline__ bool list_query(const KParams &P, const MeshView &M, 
     return true;
 }
 
+// The transport's query over the cell lists, one loop for both cases (one inlined copy of
+// the triangle test instead of two):
+//   * the step stays within the photon's own widened cell (word: its list word, not
+//     dense; bound <= g_margin + distance to the cell's faces - g_eps): that cell's list
+//     alone decides it, and `safe` is raised to the plane-distance bound of list_query;
+//   * otherwise the lists of the cells the segment's box covers (at most kLocalMaxCells),
+//     as cell_query; longer segments and dense cells go to the BVH.  The bound of the own
+//     list would not outlast such a step (it is at most that list's reach), so `safe`
+//     stays as it is.
+// Same candidates, test and tie-break as list_query / cell_query: the same hit.
+template <int STACK = kStackDepth>
+__device__ __forceinline__ int grid_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
+                                          uint32_t word, float &t_out, float &safe, bool &used_bvh)
+{
+    used_bvh = true;
+    if (!P.cell_refs) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
+    const int nx = P.g_nx, ny = P.g_ny, nz = P.g_nz;
+    const bool listed = !(word & kCellEmpty) && ((word >> 24) & 127u) != kCellDense;
+    const bool own = listed && bound <= P.g_margin + cell_face_distance(P, p.x, p.y, p.z) - P.g_eps;
+    int x0, x1, y0, y1, z0, z1;
+    if (own) {
+        x0 = x1 = (int)floorf((p.x - P.g_ox) * P.g_inv_h);
+        y0 = y1 = (int)floorf((p.y - P.g_oy) * P.g_inv_h);
+        z0 = z1 = (int)floorf((p.z - P.g_oz) * P.g_inv_h);
+    } else {
+        if (!(bound < kNoHit)) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
+        const float e = P.g_eps;
+        const float qx = p.x + bound * v.x, qy = p.y + bound * v.y, qz = p.z + bound * v.z;
+        x0 = min(max((int)floorf((fminf(p.x, qx) - e - P.g_ox) * P.g_inv_h), 0), nx - 1);
+        x1 = min(max((int)floorf((fmaxf(p.x, qx) + e - P.g_ox) * P.g_inv_h), 0), nx - 1);
+        y0 = min(max((int)floorf((fminf(p.y, qy) - e - P.g_oy) * P.g_inv_h), 0), ny - 1);
+        y1 = min(max((int)floorf((fmaxf(p.y, qy) + e - P.g_oy) * P.g_inv_h), 0), ny - 1);
+        z0 = min(max((int)floorf((fminf(p.z, qz) - e - P.g_oz) * P.g_inv_h), 0), nz - 1);
+        z1 = min(max((int)floorf((fmaxf(p.z, qz) + e - P.g_oz) * P.g_inv_h), 0), nz - 1);
+        if ((x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1) > kLocalMaxCells)
+            return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
+    }
+    float best = bound, s = own ? P.g_margin + cell_face_distance(P, p.x, p.y, p.z) - P.g_eps : 0.0f;
+    int bid = 0x7fffffff;
+    for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y)
+            for (int x = x0; x <= x1; ++x) {
+                const uint32_t w = own ? word : __ldg(P.cell_word + ((int64_t)z * ny + y) * nx + x);
+                if (w & kCellEmpty) continue;
+                uint32_t cnt = (w >> 24) & 127u;
+                if (cnt == kCellDense) return query_nearest<STACK>(M, p, v, ref_tri, bound, t_out);
+                if (!LP_IN_RANGE(M.dbg, (int64_t)(w & 0xffffffu) + cnt - 1, P.n_cell_refs)) {
+                    cnt = 0;
+                    s = 0.0f;
+                }
+                const int32_t *r = P.cell_refs + (w & 0xffffffu);
+                for (uint32_t k = 0; k < cnt; ++k) test_tri_safe(M, __ldg(r + k), p, v, ref_tri, best, bid, s);
+            }
+    used_bvh = false;
+    if (own) safe = fmaxf(safe, ref_tri >= 0 ? 0.0f : fmaxf(s - P.g_eps, 0.0f));
+    if (bid == 0x7fffffff) {
+        t_out = kNoHit;
+        return -1;
+    }
+    t_out = best;
+    return bid;
+}
+
 }  // namespace lp

@@ -570,22 +570,12 @@ __device__ __forceinline__ int query_step(const KParams &P, const MeshView &M, c
         cnt.bvh++;
         return tri;
     }
-    const uint32_t word = pd.word;
-    bool done = false;
-    // an empty cell: pd.safe_here holds its bound, which the step exceeds; a dense cell,
-    // or a grid without lists: the carried bound stays
-    if (!(word & kCellEmpty) && P.cell_refs && ((word >> 24) & 127u) != kCellDense) {
-        // the cell's own list: a bound from the planes of its triangles, and the
-        // query itself when the step stays inside the widened cell
-        done = list_query(P, M, p, v, ph.refTri, pd.reach, word, thit, tri, pd.safe_here);
-        if (done) cnt.query++;
-    }
-    if (!done) {
-        bool used_bvh;
-        tri = cell_query<STACK>(P, M, p, v, ph.refTri, pd.reach, thit, used_bvh);
-        cnt.query++;
-        cnt.bvh += used_bvh ? 1u : 0u;
-    }
+    // an empty cell: pd.safe_here holds its bound, which the step exceeds; a listed cell
+    // raises it from the planes of its triangles when its list decides the step
+    bool used_bvh;
+    tri = grid_query<STACK>(P, M, p, v, ph.refTri, pd.reach, pd.word, thit, pd.safe_here, used_bvh);
+    cnt.query++;
+    cnt.bvh += used_bvh ? 1u : 0u;
     return tri;
 }
 
