@@ -451,51 +451,22 @@ __device__ __forceinline__ int cell_query(const KParams &P, const MeshView &M, V
     return bid;
 }
 
-// The query answered from the list of p's own cell (word: a list word, not dense),
-// together with a lower bound `safe` of the distance from p to every triangle of the
-// mesh.  The list holds every triangle touching the cell widened by g_margin + g_eps, so
-// an unlisted triangle lies at least g_margin + dface from p (dface: distance from p to
-// the cell's faces), and no segment from p of length <= reach = g_margin + dface - g_eps
-// can reach one.  For listed triangles the bound is their plane distance.  On a
-// triangle (ref_tri >= 0) the bound is 0.  safe comes in holding a lower bound already
-// known (the photon's carried one) and leaves holding the larger of the two.  Returns
-// false, with safe still valid, when bound > reach: the list alone does not decide the
-// query then.
-__device__ __forceinline__ bool list_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
-                                           uint32_t word, float &t_out, int &tri_out, float &safe)
-{
-    const float reach = P.g_margin + cell_face_distance(P, p.x, p.y, p.z) - P.g_eps;
-    uint32_t cnt = (word >> 24) & 127u;
-    const int32_t *r = P.cell_refs + (word & 0xffffffu);
-    float best = bound, s = reach;
-    if (!LP_IN_RANGE(M.dbg, (int64_t)(word & 0xffffffu) + cnt - 1, P.n_cell_refs)) {
-        cnt = 0;
-        s = 0.0f;
-    }
-    int bid = 0x7fffffff;
-    for (uint32_t k = 0; k < cnt; ++k) test_tri_safe(M, __ldg(r + k), p, v, ref_tri, best, bid, s);
-    safe = fmaxf(safe, ref_tri >= 0 ? 0.0f : fmaxf(s - P.g_eps, 0.0f));
-    if (!(bound <= reach)) return false;
-    if (bid == 0x7fffffff) {
-        t_out = kNoHit;
-        tri_out = -1;
-    } else {
-        t_out = best;
-        tri_out = bid;
-    }
-    return true;
-}
-
 // The transport's query over the cell lists, one loop for both cases (one inlined copy of
-// the triangle test instead of two):
+// the triangle test):
 //   * the step stays within the photon's own widened cell (word: its list word, not
-//     dense; bound <= g_margin + distance to the cell's faces - g_eps): that cell's list
-//     alone decides it, and `safe` is raised to the plane-distance bound of list_query;
+//     dense): that cell's list alone decides it.  The list holds every triangle touching
+//     the cell widened by g_margin + g_eps, so an unlisted triangle lies at least
+//     g_margin + dface from p (dface: distance from p to the cell's faces), and no
+//     segment from p of length <= reach = g_margin + dface - g_eps can reach one.  `safe`
+//     (coming in with a lower bound already known, the photon's carried one) is raised to
+//     a lower bound of the distance from p to every triangle: reach for the unlisted ones,
+//     their plane distance (test_tri_safe) for the listed ones, 0 on a triangle
+//     (ref_tri >= 0);
 //   * otherwise the lists of the cells the segment's box covers (at most kLocalMaxCells),
 //     as cell_query; longer segments and dense cells go to the BVH.  The bound of the own
 //     list would not outlast such a step (it is at most that list's reach), so `safe`
 //     stays as it is.
-// Same candidates, test and tie-break as list_query / cell_query: the same hit.
+// Same candidates, test and tie-break as cell_query and the BVH: the same hit.
 template <int STACK = kStackDepth>
 __device__ __forceinline__ int grid_query(const KParams &P, const MeshView &M, V3 p, V3 v, int ref_tri, float bound,
                                           uint32_t word, float &t_out, float &safe, bool &used_bvh)
